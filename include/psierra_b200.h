@@ -1,0 +1,145 @@
+/*
+ * psierra_b200: C ABI of the B200 (sm_100a) Tet4/Tet10 Total-Lagrangian NeoHookean
+ * element-evaluation and global-assembly library.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status (PSX_OK
+ * on success) and never allocates device memory: the caller owns every buffer.
+ * Pointers documented as "device" must be CUDA device (or managed) memory of the
+ * current device; "host" pointers are ordinary host memory.  Work is enqueued on
+ * the given stream and is asynchronous unless stated otherwise.
+ *
+ * Reference interfaces replaced (tanadul-s/psierra, file:line):
+ *   psx_graph_count / psx_graph_fill / psx_csr_pattern
+ *       -> utility/indexing.py:35-59 compute_element_dofs,
+ *          utility/assembly.py:6-34 create_coo_sparsity_indices and the index
+ *          structure of utility/assembly.py:75-76 coo_matrix(...).tocsr()
+ *   psx_tet4_assemble (PSX_WANT_F)  -> domain/solid.py:230-274 assemble_internal_forces
+ *          (element/tet4_total_lagrangian.py:77-139 + utility/assembly.py:79-108)
+ *   psx_tet4_assemble (PSX_WANT_K)  -> domain/solid.py:280-325 assemble_tangent_stiffness_matrix
+ *          (element/tet4_total_lagrangian.py:77-139 + utility/assembly.py:37-76)
+ *   psx_tet4_assemble (PSX_LINEAR)  -> domain/solid.py:172-207 assemble_stiffness_matrix
+ *          (element/tet4_base.py:129-136)
+ *   psx_tet10_assemble              -> the same three, element/tet10_total_lagrangian.py:63-136
+ *          and element/tet10_base.py:310-342
+ *   psx_tet4_kv                     -> K_T(u) @ v with the assembled reference K_T
+ *   psx_pcg                         -> solver/sparse_linear_solver.py:37-68
+ *          ConjugateGradientSolver.solve (Jacobi-preconditioned CG)
+ */
+#ifndef PSIERRA_B200_H
+#define PSIERRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes */
+#define PSX_OK 0
+#define PSX_ERR_ARG 1           /* invalid argument (null pointer, bad size) */
+#define PSX_ERR_CUDA 2          /* a CUDA launch or copy failed */
+#define PSX_ERR_LIMIT 3         /* mesh exceeds a documented kernel limit */
+
+/* Assembly request bits (psx_tet4_assemble / psx_tet10_assemble `mode`) */
+#define PSX_WANT_F 1            /* internal force vector f_int(u) */
+#define PSX_WANT_K 2            /* tangent stiffness K_T(u) values in the CSR pattern */
+#define PSX_LINEAR 4            /* small-strain stiffness from (lambda, mu); ignores u */
+
+/* Precision of the element tangent (`precision`) */
+#define PSX_FP64 0              /* everything in FP64, K values stored as double */
+#define PSX_FP32_MIXED 1        /* f_int, det F and ln J in FP64; K_T in FP32, stored as float */
+
+/* Largest node degree (distinct neighbours incl. itself) psx_tet4_assemble accepts. */
+#define PSX_TET4_MAX_DEGREE 64
+
+/*
+ * Status block written by the element kernels (device memory, psx_status_bytes()
+ * bytes, zero it before a call).  Layout: int32 n_inverted, int32 n_bad_volume,
+ * int32 first_bad_key (INT32_MAX - lowest bad element index, 0 if none),
+ * int32 n_not_finite, int32 iters, int32 flags, double value.
+ * An element is "bad" when its reference volume det is <= 0 (n_bad_volume) or
+ * det F <= 0 (n_inverted): the two conditions on which the reference raises
+ * ValueError (element/tet4_base.py:56-61, element/tet4_total_lagrangian.py:110-112).
+ */
+size_t psx_status_bytes(void);
+
+/* ---- Sparsity pattern (host memory, once per mesh) ------------------------- */
+
+/*
+ * Node graph of a mesh with `npe` nodes per element (4 or 10), connectivity
+ * `conn` (host, E x npe, row-major, int64, node ids in [0, N)).
+ *   nbr_ptr (host, N+1): prefix sums of node degrees (distinct neighbours incl. self)
+ *   inc_ptr (host, N+1): prefix sums of node -> element incidences
+ * Returns PSX_ERR_LIMIT if 9 * sum(deg) does not fit int32.
+ */
+int psx_graph_count(const int64_t* conn, int64_t E, int npe, int64_t N,
+                    int32_t* nbr_ptr, int32_t* inc_ptr);
+
+/*
+ * Fill the node graph (host): nbr (sum deg) sorted neighbour lists; inc_elem
+ * (E*npe) incident elements of each node in ascending element order; inc_code
+ * (E*npe): for Tet4, bits 0-1 = local index of the node in the element and bits
+ * 2+7b..8+7b = rank of element node b in the node's neighbour list (ranks < 128);
+ * for Tet10 the local index only.
+ */
+int psx_graph_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
+                   const int32_t* nbr_ptr, const int32_t* inc_ptr,
+                   int32_t* nbr, int32_t* inc_elem, uint32_t* inc_code);
+
+/*
+ * Canonical CSR pattern of the assembled 3N x 3N matrix (host): indptr (3N+1),
+ * indices (9*sum deg), identical to scipy's coo_matrix((data,(rows,cols))).tocsr()
+ * index arrays for the reference's rows/cols (sorted columns, duplicates merged).
+ * Row 3i+k of node i starts at 9*nbr_ptr[i] + 3*deg_i*k.
+ */
+int psx_csr_pattern(int64_t N, const int32_t* nbr_ptr, const int32_t* nbr,
+                    int32_t* indptr, int32_t* indices);
+
+/*
+ * Per neighbour-block gather lists (host) used by the Tet10 path: for the block
+ * (node i, neighbour rank r) at entry q = nbr_ptr[i] + r, blk_src[blk_ptr[q] ..
+ * blk_ptr[q+1]) lists (e*npe + a)*npe + b for every element e containing node i at
+ * local index a and the neighbour at local index b, in ascending element order.
+ * blk_ptr has sum(deg)+1 entries, blk_src E*npe*npe.  PSX_ERR_LIMIT if E*npe*npe
+ * does not fit int32.
+ */
+int psx_block_lists(const int64_t* conn, int64_t E, int npe, int64_t N,
+                    const int32_t* nbr_ptr, const int32_t* nbr,
+                    int32_t* blk_ptr, int32_t* blk_src);
+
+/* ---- Tet4 element kernels (device) ----------------------------------------- */
+
+/*
+ * Tet4 Total-Lagrangian NeoHookean assembly (replaces the element loops of
+ * domain/solid.py:230-325 and the COO->CSR / np.add.at scatter).
+ *   conn (device, E x 4 int32), X, u (device, N x 3 double; u ignored for PSX_LINEAR)
+ *   mu_e, kappa_e (device, E doubles) per-element moduli, or NULL to use mu, kappa
+ *   lam: Lame lambda for PSX_LINEAR (with mu)
+ *   graph arrays from psx_graph_fill (device copies), max_degree = max node degree
+ *   f_out (device, 3N doubles) when mode has PSX_WANT_F
+ *   k_out (device, nnz values: double for PSX_FP64, float for PSX_FP32_MIXED)
+ *   status (device, psx_status_bytes(), zeroed by the caller)
+ * Deterministic: every output value is a fixed-order sum; no atomics touch f or K.
+ */
+int psx_tet4_assemble(const int32_t* conn, const double* X, const double* u,
+                      const double* mu_e, const double* kappa_e,
+                      double mu, double kappa, double lam,
+                      int64_t E, int64_t N,
+                      const int32_t* nbr_ptr, const int32_t* inc_ptr,
+                      const int32_t* inc_elem, const uint32_t* inc_code, int max_degree,
+                      int mode, int precision,
+                      double* f_out, void* k_out, void* status, void* stream);
+
+/*
+ * Reference det (of [1 X], = 6 V) and det F of one element, written to out2
+ * (device, 2 doubles).  Used to word the inversion error of a failed call.
+ */
+int psx_tet4_element_dets(const int32_t* conn, const double* X, const double* u,
+                          int64_t e, double* out2, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSIERRA_B200_H */

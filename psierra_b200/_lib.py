@@ -1,0 +1,83 @@
+"""ctypes binding of ``libpsierra_b200.so`` (the C ABI declared in ``include/psierra_b200.h``).
+
+The library is required: importing the product path without it raises, and there
+is no CPU fallback for any kernel.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpsierra_b200.so")
+
+PSX_OK = 0
+PSX_ERR_ARG = 1
+PSX_ERR_CUDA = 2
+PSX_ERR_LIMIT = 3
+
+PSX_WANT_F = 1
+PSX_WANT_K = 2
+PSX_LINEAR = 4
+
+PSX_FP64 = 0
+PSX_FP32_MIXED = 1
+
+PSX_TET4_MAX_DEGREE = 64
+
+_ERRORS = {
+    PSX_ERR_ARG: "invalid argument",
+    PSX_ERR_CUDA: "CUDA launch or copy failed",
+    PSX_ERR_LIMIT: "mesh exceeds a kernel limit",
+}
+
+_p = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int
+_f64 = ctypes.c_double
+
+# name -> (argtypes); every function returns int except psx_status_bytes (size_t)
+SIGNATURES: dict[str, list] = {
+    "psx_graph_count": [_p, _i64, _i32, _i64, _p, _p],
+    "psx_graph_fill": [_p, _i64, _i32, _i64, _p, _p, _p, _p, _p],
+    "psx_csr_pattern": [_i64, _p, _p, _p, _p],
+    "psx_block_lists": [_p, _i64, _i32, _i64, _p, _p, _p, _p],
+    "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i64, _i64, _p, _p, _p, _p, _i32,
+                          _i32, _i32, _p, _p, _p, _p],
+    "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load (once) and return the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m psierra_b200.build` "
+                "(psierra_b200 has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, argtypes in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = argtypes
+            fn.restype = ctypes.c_int
+        L.psx_status_bytes.argtypes = []
+        L.psx_status_bytes.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != PSX_OK:
+        raise RuntimeError(f"{what} failed: {_ERRORS.get(rc, 'error')} (code {rc})")
+
+
+def ptr(t) -> int | None:
+    """Raw address of a torch tensor or numpy array (None stays NULL)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data

@@ -1,0 +1,158 @@
+"""Device-resident assembler: mesh, pattern and material on the GPU; one call per sweep.
+
+``GPUAssembler`` owns the device copies of a mesh (coordinates, connectivity, node
+graph, CSR pattern) and of its material, and launches the element kernels of
+``libpsierra_b200.so`` on the current torch stream.  Inputs and outputs are torch
+tensors on the device; the drop-in element classes in ``psierra_b200.element`` add
+the host <-> device copies the reference API needs.
+
+Error behaviour matches the reference: an element with non-positive reference
+volume raises ``ValueError("Negative or zero element volume detected ...")``
+(psierra ``element/tet4_base.py:56-61``) and an inverted element raises
+``ValueError("Element inversion detected: det(F) = ... <= 0.")``
+(``element/tet4_total_lagrangian.py:110-112``), for the lowest-index bad element,
+as the reference's element loop would.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from psierra_b200 import _lib
+from psierra_b200._lib import check, lib, ptr
+from psierra_b200.material import material_moduli
+from psierra_b200.pattern import MeshPattern
+
+PRECISIONS = {"fp64": _lib.PSX_FP64, "fp32-mixed": _lib.PSX_FP32_MIXED}
+
+
+def _stream_handle() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class GPUAssembler:
+    """Assembler for one Tet4 or Tet10 mesh with a NeoHookean material (constant or per element)."""
+
+    def __init__(self, nodes: np.ndarray, elements: np.ndarray, material, precision: str = "fp64",
+                 device=None, pattern: MeshPattern | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("psierra_b200 requires a CUDA device (no CPU fallback)")
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
+        lib()  # fail loudly now if the library is missing
+        self.device = torch.device(device if device is not None else "cuda")
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        self.pattern = pattern if pattern is not None else MeshPattern(elements, nodes.shape[0])
+        self.npe = self.pattern.npe
+        self.n_nodes = self.pattern.n_nodes
+        self.n_elements = self.pattern.n_elements
+        self.precision = precision
+        self.dev = self.pattern.device(self.device)
+        self.X = torch.from_numpy(nodes).to(self.device)
+        nbytes = int(lib().psx_status_bytes())
+        self.status = torch.zeros((nbytes + 3) // 4, dtype=torch.int32, device=self.device)
+        self._dets = torch.zeros(2, dtype=torch.float64, device=self.device)
+        self.set_material(material)
+
+    # ------------------------------------------------------------------ material
+    def set_material(self, material) -> None:
+        self.material = material
+        mu, kappa, lam = material_moduli(material)
+        self.mu, self.kappa, self.lam = mu, kappa, lam
+        self.rho = float(getattr(material, "mass_density", 0.0) or 0.0)
+        self.mu_e = self._per_element(getattr(material, "mu_e", None))
+        self.kappa_e = self._per_element(getattr(material, "kappa_e", None))
+
+    def _per_element(self, a):
+        if a is None:
+            return None
+        t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.asarray(a, dtype=np.float64))
+        t = t.to(device=self.device, dtype=torch.float64).contiguous()
+        if t.numel() != self.n_elements:
+            raise ValueError(f"per-element modulus has {t.numel()} entries, mesh has {self.n_elements} elements")
+        return t
+
+    # ------------------------------------------------------------------ buffers
+    @property
+    def nnz(self) -> int:
+        return self.pattern.nnz
+
+    def k_dtype(self, precision: str | None = None):
+        return torch.float64 if (precision or self.precision) == "fp64" else torch.float32
+
+    def new_f(self) -> torch.Tensor:
+        return torch.empty(3 * self.n_nodes, dtype=torch.float64, device=self.device)
+
+    def new_k(self, precision: str | None = None) -> torch.Tensor:
+        return torch.empty(self.nnz, dtype=self.k_dtype(precision), device=self.device)
+
+    # ------------------------------------------------------------------ kernels
+    def assemble(self, u: torch.Tensor | None, want_f: bool = True, want_k: bool = True,
+                 precision: str | None = None, f_out: torch.Tensor | None = None,
+                 k_out: torch.Tensor | None = None, check_status: bool = True, linear: bool = False):
+        """One sweep over all elements.  Returns ``(f, k)``; either may be None.
+
+        ``u`` is the ``(N, 3)`` (or ``(3N,)``) float64 displacement on the device.
+        ``k`` holds the CSR values in ``pattern.indptr``/``indices`` order (float64,
+        or float32 for ``precision="fp32-mixed"``).  With ``linear=True`` the
+        small-strain stiffness of the reference configuration is assembled instead
+        (``u`` is ignored).
+        """
+        prec = precision or self.precision
+        if prec not in PRECISIONS:
+            raise ValueError(f"unknown precision {prec!r}")
+        if self.npe != 4:
+            raise NotImplementedError("Tet10 assembly is provided by psierra_b200.tet10")
+        if linear:
+            mode = _lib.PSX_LINEAR
+            want_f, want_k = False, True
+        else:
+            mode = (_lib.PSX_WANT_F if want_f else 0) | (_lib.PSX_WANT_K if want_k else 0)
+            if mode == 0:
+                raise ValueError("nothing requested")
+            u = self._check_u(u)
+        if want_f and f_out is None:
+            f_out = self.new_f()
+        if want_k and k_out is None:
+            k_out = self.new_k(prec)
+        if want_k and k_out.dtype != self.k_dtype(prec):
+            raise ValueError(f"k_out must be {self.k_dtype(prec)} for precision {prec}")
+        self.status.zero_()
+        d = self.dev
+        rc = lib().psx_tet4_assemble(
+            ptr(d["conn"]), ptr(self.X), ptr(u) if not linear else None,
+            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam,
+            self.n_elements, self.n_nodes, ptr(d["nbr_ptr"]), ptr(d["inc_ptr"]), ptr(d["inc_elem"]),
+            ptr(d["inc_code"]), self.pattern.max_degree, mode, PRECISIONS[prec],
+            ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(self.status),
+            _stream_handle())
+        check(rc, "psx_tet4_assemble")
+        if check_status:
+            self.raise_on_bad_elements(u)
+        return (f_out if want_f else None), (k_out if want_k else None)
+
+    def _check_u(self, u: torch.Tensor) -> torch.Tensor:
+        if not isinstance(u, torch.Tensor) or u.device != self.X.device or u.dtype != torch.float64:
+            raise ValueError("u must be a float64 tensor on the assembler's device")
+        if u.numel() != 3 * self.n_nodes:
+            raise ValueError(f"u has {u.numel()} entries, expected {3 * self.n_nodes}")
+        return u.contiguous()
+
+    # ------------------------------------------------------------------ status
+    def status_counts(self) -> tuple[int, int, int]:
+        """(n_inverted, n_bad_volume, first_bad_element or -1) of the last sweep (synchronises)."""
+        s = self.status[:3].cpu().numpy()
+        first = int(0x7FFFFFFF - int(s[2])) if s[2] != 0 else -1
+        return int(s[0]), int(s[1]), first
+
+    def raise_on_bad_elements(self, u: torch.Tensor | None) -> None:
+        n_inv, n_vol, first = self.status_counts()
+        if n_inv == 0 and n_vol == 0:
+            return
+        check(lib().psx_tet4_element_dets(ptr(self.dev["conn"]), ptr(self.X), ptr(u), first,
+                                          ptr(self._dets), _stream_handle()), "psx_tet4_element_dets")
+        detA, J = (float(v) for v in self._dets.cpu().numpy())
+        if not detA > 0.0:
+            raise ValueError(
+                f"Negative or zero element volume detected (det(A) = {detA}). Check element vertex ordering.")
+        raise ValueError(f"Element inversion detected: det(F) = {J:.4e} <= 0.")

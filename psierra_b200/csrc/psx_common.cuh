@@ -1,0 +1,174 @@
+// Shared device code for the Tet4/Tet10 Total-Lagrangian NeoHookean kernels.
+//
+// Element math follows pSierra's Tet4/Tet10 TL elements and NeoHookean material
+// (psierra element/tet4_total_lagrangian.py:77-139, element/tet10_total_lagrangian.py:63-136,
+// material/neohookean.py:55-122) in a closed, symmetry-exploiting form:
+//
+//   l  = sum_b u_b g_b^T          (displacement gradient, g_b = grad N_b)
+//   F  = I + l,  J - 1 = tr l + ((tr l)^2 - tr l^2)/2 + det l   (no cancellation at small l)
+//   ln J = log1p(J - 1),  phi = mu J^(-2/3),  beta = kappa ln J
+//   S  = C^-1 (2 phi dev E + beta I),  E = (l + l^T + l^T l)/2     (== the reference's
+//        phi (I - I1/3 C^-1) + beta C^-1, without its O(mu) cancellation)
+//   f_a = V F S g_a
+//   K_ab = V [ A p_a p_b^T + hb p_b p_a^T + c (p_a q_b^T + q_a p_b^T) + phi (g_a . g_b) I ]
+//        with p_a = F^-T g_a, q_a = F g_a, A = kappa + 2/9 phi I1, hb = phi I1/3 - beta,
+//        c = -2/3 phi.
+//
+// K_ab equals B_a^T C_voigt B_b V + G_a^T (I (x) S) G_b V of the reference: the
+// C^-1 (x) C^-1, the symmetrised C^-1 product and the C^-1 (x) I terms of the 4th-order
+// tangent contract with B = sym(F^T grad N) to the three outer products, and the
+// p_a.p_b parts of the symmetrised term and of the geometric term cancel exactly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "psierra_b200.h"
+
+namespace psx {
+
+struct Mat3 {
+  double m[3][3];
+};
+
+__device__ __forceinline__ double det3(const double a[3][3]) {
+  return a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+         a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+         a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+}
+
+// Inverse through the adjugate; returns the determinant.
+__device__ __forceinline__ double inv3(const double a[3][3], double r[3][3]) {
+  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  double c01 = a[0][2] * a[2][1] - a[0][1] * a[2][2];
+  double c02 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
+  double c10 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+  double c11 = a[0][0] * a[2][2] - a[0][2] * a[2][0];
+  double c12 = a[0][2] * a[1][0] - a[0][0] * a[1][2];
+  double c20 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  double c21 = a[0][1] * a[2][0] - a[0][0] * a[2][1];
+  double c22 = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+  double det = a[0][0] * c00 + a[0][1] * c10 + a[0][2] * c20;
+  double id = 1.0 / det;
+  r[0][0] = c00 * id; r[0][1] = c01 * id; r[0][2] = c02 * id;
+  r[1][0] = c10 * id; r[1][1] = c11 * id; r[1][2] = c12 * id;
+  r[2][0] = c20 * id; r[2][1] = c21 * id; r[2][2] = c22 * id;
+  return det;
+}
+
+// Kinematic + constitutive state of one integration point, everything in FP64.
+struct PointState {
+  double F[3][3];     // deformation gradient
+  double Finv[3][3];  // F^-1
+  double P[3][3];     // first Piola-Kirchhoff stress F S
+  double Jm1;         // J - 1 (compensated)
+  double phi;         // mu J^(-2/3)
+  double beta;        // kappa ln J
+  double I1;          // tr C
+};
+
+// Constitutive update from the displacement gradient l (3x3, FP64).
+// neohookean.py:74-92 restated without cancellation (see the header comment).
+__device__ __forceinline__ void neohookean_point(const double l[3][3], double mu, double kappa,
+                                                 PointState& s) {
+  double trl = l[0][0] + l[1][1] + l[2][2];
+  double trl2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) trl2 += l[i][k] * l[k][i];
+  s.Jm1 = trl + 0.5 * (trl * trl - trl2) + det3(l);
+  double lnJ = log1p(s.Jm1);
+  s.phi = mu * exp((-2.0 / 3.0) * lnJ);
+  s.beta = kappa * lnJ;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) s.F[i][j] = (i == j ? 1.0 : 0.0) + l[i][j];
+  inv3(s.F, s.Finv);
+  // Green-Lagrange strain E = (l + l^T + l^T l) / 2 and its deviator.
+  double E[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double ltl = l[0][i] * l[0][j] + l[1][i] * l[1][j] + l[2][i] * l[2][j];
+      E[i][j] = 0.5 * (l[i][j] + l[j][i] + ltl);
+    }
+  double trE = E[0][0] + E[1][1] + E[2][2];
+  s.I1 = 3.0 + 2.0 * trE;
+  // T = 2 phi dev E + beta I
+  double T[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      T[i][j] = 2.0 * s.phi * (E[i][j] - (i == j ? trE / 3.0 : 0.0)) + (i == j ? s.beta : 0.0);
+  // C^-1 = F^-1 F^-T
+  double Ci[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      Ci[i][j] = s.Finv[i][0] * s.Finv[j][0] + s.Finv[i][1] * s.Finv[j][1] + s.Finv[i][2] * s.Finv[j][2];
+  // S = C^-1 T (symmetric: C^-1 and dev E commute), P = F S
+  double S[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) {
+      double v = Ci[i][0] * T[0][j] + Ci[i][1] * T[1][j] + Ci[i][2] * T[2][j];
+      S[i][j] = v;
+      S[j][i] = v;
+    }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      s.P[i][j] = s.F[i][0] * S[0][j] + s.F[i][1] * S[1][j] + s.F[i][2] * S[2][j];
+}
+
+// Tangent coefficients with the integration weight folded in.
+template <typename T>
+struct TangentCoef {
+  T A, hb, c, phi;
+};
+
+template <typename T>
+__device__ __forceinline__ TangentCoef<T> tangent_coef(const PointState& s, double kappa, double w) {
+  TangentCoef<T> t;
+  t.A = (T)(w * (kappa + (2.0 / 9.0) * s.phi * s.I1));
+  t.hb = (T)(w * (s.phi * s.I1 / 3.0 - s.beta));
+  t.c = (T)(w * (-(2.0 / 3.0) * s.phi));
+  t.phi = (T)(w * s.phi);
+  return t;
+}
+
+// Status words written by every element kernel (device side).  Counters are
+// reset with a plain memset; `first_bad_key` stores INT32_MAX - e so that an
+// atomicMax picks the lowest element index and a zeroed word means "none".
+struct Status {
+  int32_t n_inverted;     // elements with det F <= 0
+  int32_t n_bad_volume;   // elements with reference det <= 0
+  int32_t first_bad_key;  // INT32_MAX - (lowest bad element index), 0 if none
+  int32_t n_not_finite;   // reserved for solver status
+  int32_t iters;          // solver iterations (PCG)
+  int32_t flags;          // solver flags
+  double value;           // solver residual or auxiliary value
+};
+
+__device__ __forceinline__ void flag_bad_element(Status* st, int64_t e, bool volume) {
+  if (volume)
+    atomicAdd(&st->n_bad_volume, 1);
+  else
+    atomicAdd(&st->n_inverted, 1);
+  atomicMax(&st->first_bad_key, (int32_t)(0x7fffffff - (int32_t)e));
+}
+
+}  // namespace psx
+
+#define PSX_CUDA_CHECK_LAUNCH()                      \
+  do {                                               \
+    cudaError_t _e = cudaGetLastError();             \
+    if (_e != cudaSuccess) return PSX_ERR_CUDA;      \
+  } while (0)

@@ -1,0 +1,196 @@
+"""Drop-in GPU elements for pSierra's ``SolidDomain`` (Tet4 / Tet10 Total Lagrangian).
+
+``SolidDomain`` delegates to its element when the element defines
+``assemble_internal_forces(mesh, displacement)``, ``assemble_tangent_stiffness_matrix
+(mesh, displacement)``, ``assemble_stiffness_matrix(mesh)`` or ``prepare_for_assembly``
+(psierra ``domain/solid.py:180-181, 238-244, 288-294``; the same hooks ``Tet4Fbar``
+uses, ``element/tet4_fbar.py:217-459``).  The classes here implement those hooks on
+the GPU, so the reference's unchanged ``SolidDomain``, ``NonlinearStaticAnalysis``,
+``DynamicRelaxationAnalysis`` and ``NonlinearDynamicAnalysis`` run on them as they are,
+and so does the mirror domain and drivers of this package.
+
+Return values follow the reference: a fresh ``(3N,)`` float64 numpy array for the
+internal forces and a canonical ``scipy.sparse.csr_matrix`` (sorted indices, int32
+index arrays identical to ``coo_matrix(...).tocsr()``) for the matrices.  In
+``precision="fp32-mixed"`` the tangent values are computed and stored in FP32 on
+the device and widened to float64 on the way out; f_int stays FP64.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as spsp
+import torch
+
+from psierra_b200.assembler import GPUAssembler
+
+
+class _HostStaging:
+    """Pinned host buffers for the per-call copies of u (in) and f / K values (out)."""
+
+    def __init__(self):
+        self._bufs: dict[tuple, torch.Tensor] = {}
+
+    def get(self, key: str, n: int, dtype) -> torch.Tensor:
+        k = (key, dtype)
+        b = self._bufs.get(k)
+        if b is None or b.numel() < n:
+            b = torch.empty(n, dtype=dtype, pin_memory=True)
+            self._bufs[k] = b
+        return b[:n]
+
+
+class _GPUElementBase:
+    """Common host <-> device plumbing of the drop-in element classes."""
+
+    supports_element_indexing: bool = True
+    _npe = 4
+
+    def __init__(self, material, precision: str = "fp64", device=None) -> None:
+        self._material = material
+        self.precision = precision
+        self.device = device
+        self._mesh = None
+        self._asm: GPUAssembler | None = None
+        self._staging = _HostStaging()
+        self._u_dev: torch.Tensor | None = None
+        self._last_u: np.ndarray | None = None
+        self._last_f: torch.Tensor | None = None
+
+    # ---------------------------------------------------------------- interface
+    @property
+    def material(self):
+        return self._material
+
+    @material.setter
+    def material(self, mat) -> None:
+        self._material = mat
+        if self._asm is not None:
+            self._asm.set_material(mat)
+        self._last_u = None
+
+    @property
+    def nodes_per_element(self) -> int:
+        return self._npe
+
+    @property
+    def dofs_per_node(self) -> int:
+        return 3
+
+    @property
+    def dofs_per_element(self) -> int:
+        return 3 * self._npe
+
+    # ---------------------------------------------------------------- setup
+    def _make_assembler(self, mesh) -> GPUAssembler:
+        return GPUAssembler(mesh.nodes, mesh.elements, self._material, precision=self.precision,
+                            device=self.device)
+
+    def _setup(self, mesh) -> GPUAssembler:
+        if self._mesh is not mesh or self._asm is None:
+            elements = np.asarray(mesh.elements)
+            if elements.ndim != 2 or elements.shape[1] != self._npe:
+                raise ValueError(f"{type(self).__name__} needs (E, {self._npe}) elements, got {elements.shape}")
+            self._asm = self._make_assembler(mesh)
+            self._mesh = mesh
+            self._u_dev = torch.empty(3 * self._asm.n_nodes, dtype=torch.float64, device=self._asm.device)
+            self._last_u = None
+        return self._asm
+
+    def prepare_for_assembly(self, mesh, displacement=None) -> None:
+        """Build (once per mesh) the device mesh, node graph and CSR pattern."""
+        self._setup(mesh)
+
+    def prepare_for_linear_assembly(self, mesh) -> None:
+        self._setup(mesh)
+
+    def _upload_u(self, displacement) -> torch.Tensor:
+        u = np.ascontiguousarray(displacement, dtype=np.float64).reshape(-1)
+        if u.size != self._u_dev.numel():
+            raise ValueError(f"displacement has {u.size} entries, expected {self._u_dev.numel()}")
+        pin = self._staging.get("u", u.size, torch.float64)
+        pin.numpy()[:] = u
+        self._u_dev.copy_(pin, non_blocking=True)
+        return self._u_dev
+
+    def _download(self, t: torch.Tensor, key: str) -> np.ndarray:
+        pin = self._staging.get(key, t.numel(), t.dtype)
+        pin.copy_(t, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return pin.numpy().astype(np.float64, copy=True)
+
+    def _csr(self, kvals: torch.Tensor) -> spsp.csr_matrix:
+        p = self._asm.pattern
+        data = self._download(kvals, "k")
+        n = p.n_dofs
+        A = spsp.csr_matrix((data, p.indices, p.indptr), shape=(n, n), copy=False)
+        A.has_sorted_indices = True
+        A.has_canonical_format = True
+        return A
+
+    # ---------------------------------------------------------------- domain hooks
+    def assemble_internal_forces(self, mesh, displacement) -> np.ndarray:
+        """f_int(u) as a fresh ``(3N,)`` array (psierra ``domain/solid.py:230-274``)."""
+        asm = self._setup(mesh)
+        u = self._upload_u(displacement)
+        f, _ = asm.assemble(u, want_f=True, want_k=False)
+        return self._download(f, "f")
+
+    def assemble_tangent_stiffness_matrix(self, mesh, displacement) -> spsp.csr_matrix:
+        """K_T(u) as a canonical CSR matrix (psierra ``domain/solid.py:280-325``)."""
+        asm = self._setup(mesh)
+        u = self._upload_u(displacement)
+        _, k = asm.assemble(u, want_f=False, want_k=True)
+        return self._csr(k)
+
+    def assemble_stiffness_matrix(self, mesh) -> spsp.csr_matrix:
+        """Small-strain K of the reference configuration (psierra ``domain/solid.py:172-207``)."""
+        asm = self._setup(mesh)
+        _, k = asm.assemble(None, linear=True)
+        return self._csr(k)
+
+    def assemble_force_and_tangent(self, mesh, displacement) -> tuple[np.ndarray, spsp.csr_matrix]:
+        """Both outputs from one fused element sweep."""
+        asm = self._setup(mesh)
+        u = self._upload_u(displacement)
+        f, k = asm.assemble(u, want_f=True, want_k=True)
+        return self._download(f, "f"), self._csr(k)
+
+    # ---------------------------------------------------------------- per-element API
+    def compute_nonlinear_force_and_tangent_stiffness(self, node_coords, u_nodes, elem_index=None, **kw):
+        """(k_tan, f_int) of one element (psierra ``element/tet4_total_lagrangian.py:77-139``).
+
+        Runs the same GPU kernel on a one-element mesh; it exists for API
+        compatibility, while the domain hooks above are the throughput path.
+        """
+        from psierra_b200.meshgen import TetMesh
+
+        X = np.asarray(node_coords, dtype=np.float64).reshape(self._npe, 3)
+        mat = self._material
+        if elem_index is not None and getattr(mat, "mu_e", None) is not None:
+            from psierra_b200.material import NeoHookeanField, _host
+
+            mat = NeoHookeanField(np.asarray(_host(mat.mu_e))[[elem_index]],
+                                  np.asarray(_host(mat.kappa_e))[[elem_index]])
+        one = type(self)(mat, precision=self.precision, device=self.device)
+        mesh = TetMesh(X, np.arange(self._npe, dtype=np.int64)[None, :])
+        f, K = one.assemble_force_and_tangent(mesh, np.asarray(u_nodes, dtype=np.float64))
+        return K.toarray(), f
+
+    def compute_linear_stiffness_matrix(self, node_coords, elem_index=None, **kw):
+        from psierra_b200.meshgen import TetMesh
+
+        X = np.asarray(node_coords, dtype=np.float64).reshape(self._npe, 3)
+        one = type(self)(self._material, precision=self.precision, device=self.device)
+        return one.assemble_stiffness_matrix(TetMesh(X, np.arange(self._npe, dtype=np.int64)[None, :])).toarray()
+
+
+class Tet4TotalLagrangian(_GPUElementBase):
+    """GPU Tet4 Total-Lagrangian element (psierra ``element/tet4_total_lagrangian.py``)."""
+
+    _npe = 4
+
+    def compute_mass_matrix(self, volume: float) -> np.ndarray:
+        """Consistent 12x12 element mass (psierra ``element/tet4_base.py:138-151``)."""
+        rho = self._material.mass_density
+        m = np.kron(np.ones((4, 4)) + np.identity(4), np.identity(3))
+        return (rho * volume / 20.0) * m

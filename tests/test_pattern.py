@@ -1,0 +1,135 @@
+"""Host-side pattern logic and the C ABI surface (CPU only).
+
+* the library loads and exports every entry point declared in ``include/*.h``;
+* the CSR index arrays equal scipy's ``coo_matrix(...).tocsr()`` of the reference's
+  COO triplets bit for bit (psierra ``utility/assembly.py:6-34, 75-76``);
+* the node-centric slot map reproduces scipy's duplicate summation exactly
+  (integer-valued element matrices, so any ordering gives the same sums);
+* the Tet10 gather lists do the same for the element-centric path.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+import scipy.sparse as spsp
+
+from conftest import ROOT
+from oracle.assembly import coo_indices, element_dofs
+from psierra_b200 import _lib, meshgen
+from psierra_b200.pattern import MeshPattern
+
+
+def declared_symbols() -> list[str]:
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        names += re.findall(r"^\s*(?:int|size_t|void)\s+(psx_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_symbols()
+    assert len(names) >= 7
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in include/ but not exported"
+    assert L.psx_status_bytes() == 32
+
+
+def _scipy_pattern(elements, n_dofs):
+    ed = element_dofs(elements)
+    r, c = coo_indices(ed)
+    return spsp.coo_matrix((np.ones(r.size), (r, c)), shape=(n_dofs, n_dofs)).tocsr(), r, c
+
+
+def _random_unstructured(seed=0):
+    """Randomly renumbered Kuhn box with shuffled element order (an 'unstructured' mesh)."""
+    rng = np.random.default_rng(seed)
+    m = meshgen.box_tet4(1.0, 0.7, 0.5, 5, 4, 3)
+    perm = rng.permutation(m.n_nodes)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(m.n_nodes)
+    els = inv[m.elements][rng.permutation(m.n_elements)]
+    return meshgen.TetMesh(m.nodes[perm], els)
+
+
+MESHES = {
+    "cfg1": lambda: meshgen.box_tet4(1.0, 0.1, 0.1, 40, 4, 4),
+    "unstructured": _random_unstructured,
+    "tet10": lambda: meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, 3, 2, 2)),
+    "single": lambda: meshgen.TetMesh(np.eye(4, 3, k=-1) + 0.0, np.array([[0, 1, 2, 3]])),
+}
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_csr_pattern_bit_exact(name):
+    m = MESHES[name]()
+    p = MeshPattern(m.elements, m.n_nodes)
+    A, _, _ = _scipy_pattern(m.elements, m.n_dofs)
+    assert p.indptr.dtype == A.indptr.dtype == np.int32
+    assert np.array_equal(p.indptr, A.indptr)
+    assert np.array_equal(p.indices, A.indices)
+    assert p.nnz == A.nnz
+
+
+@pytest.mark.parametrize("name", ["cfg1", "unstructured", "single"])
+def test_tet4_slot_map_reproduces_coo_sum(name):
+    m = MESHES[name]()
+    p = MeshPattern(m.elements, m.n_nodes)
+    E = m.n_elements
+    rng = np.random.default_rng(1)
+    kl = rng.integers(-1000, 1000, size=(E, 12, 12)).astype(np.float64)
+    _, r, c = _scipy_pattern(m.elements, m.n_dofs)
+    B = spsp.coo_matrix((kl.ravel(), (r, c)), shape=(m.n_dofs,) * 2).tocsr()
+    vals = np.zeros(p.nnz)
+    for i in range(m.n_nodes):
+        deg = p.nbr_ptr[i + 1] - p.nbr_ptr[i]
+        base = 9 * p.nbr_ptr[i]
+        for s in range(p.inc_ptr[i], p.inc_ptr[i + 1]):
+            e, code = p.inc_elem[s], int(p.inc_code[s])
+            a = code & 3
+            assert m.elements[e, a] == i
+            for b in range(4):
+                rb = (code >> (2 + 7 * b)) & 127
+                blk = kl[e, 3 * a:3 * a + 3, 3 * b:3 * b + 3]
+                for k in range(3):
+                    vals[base + 3 * deg * k + 3 * rb: base + 3 * deg * k + 3 * rb + 3] += blk[k]
+    assert np.array_equal(vals, B.data)
+
+
+def test_block_lists_reproduce_coo_sum():
+    m = MESHES["tet10"]()
+    p = MeshPattern(m.elements, m.n_nodes)
+    blk_ptr, blk_src = p.block_lists()
+    E, npe = m.elements.shape
+    rng = np.random.default_rng(2)
+    kl = rng.integers(-1000, 1000, size=(E, 3 * npe, 3 * npe)).astype(np.float64)
+    _, r, c = _scipy_pattern(m.elements, m.n_dofs)
+    B = spsp.coo_matrix((kl.ravel(), (r, c)), shape=(m.n_dofs,) * 2).tocsr()
+    vals = np.zeros(p.nnz)
+    for i in range(m.n_nodes):
+        deg = p.nbr_ptr[i + 1] - p.nbr_ptr[i]
+        for rr in range(deg):
+            q = p.nbr_ptr[i] + rr
+            srcs = blk_src[blk_ptr[q]:blk_ptr[q + 1]]
+            assert np.all(np.diff(srcs // (npe * npe)) > 0)  # ascending element order
+            for s in srcs:
+                e, a, b = s // (npe * npe), (s // npe) % npe, s % npe
+                assert m.elements[e, a] == i and m.elements[e, b] == p.nbr[q]
+                blk = kl[e, 3 * a:3 * a + 3, 3 * b:3 * b + 3]
+                for k in range(3):
+                    o = 9 * p.nbr_ptr[i] + 3 * deg * k + 3 * rr
+                    vals[o:o + 3] += blk[k]
+    assert np.array_equal(vals, B.data)
+
+
+def test_pattern_rejects_bad_connectivity():
+    els = np.array([[0, 1, 2, 7]], dtype=np.int64)
+    with pytest.raises(RuntimeError, match="invalid argument"):
+        MeshPattern(els, 4)
+    with pytest.raises(ValueError):
+        MeshPattern(np.zeros((3, 5), dtype=np.int64), 8)
