@@ -98,9 +98,10 @@ tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
   const int i0 = inc_ptr[node], i1 = inc_ptr[node + 1];
   const int nb0 = nbr_ptr[node], deg = nbr_ptr[node + 1] - nb0;
 
-  double acc0[9], acc1[9], facc[3];
+  KT acc0[9], acc1[9];
+  double facc[3];
 #pragma unroll
-  for (int j = 0; j < 9; ++j) acc0[j] = acc1[j] = 0.0;
+  for (int j = 0; j < 9; ++j) acc0[j] = acc1[j] = (KT)0;
   facc[0] = facc[1] = facc[2] = 0.0;
 
   for (int c0 = i0; c0 < i1; c0 += 32) {
@@ -120,19 +121,30 @@ tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
       if (a == 0 && !(G.detD > 0.0)) flag_bad_element(st, e, true);
       sCode[warp][lane] = code;
 
+      // Own-node vectors are picked with selects so nothing is indexed at run time.
+      double gad[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        gad[k] = a == 0 ? G.g[0][k] : a == 1 ? G.g[1][k] : a == 2 ? G.g[2][k] : G.g[3][k];
+      KT gk[4][3];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) gk[b][k] = (KT)G.g[b][k];
+      const KT ga[3] = {(KT)gad[0], (KT)gad[1], (KT)gad[2]};
+
       if constexpr (kLinear) {
         // tet4_base.py:129-136: K_ab = V [lam g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I]
         const KT Vl = (KT)(G.V * lam0), Vm = (KT)(G.V * mu0);
-        KT ga[3] = {(KT)G.g[a][0], (KT)G.g[a][1], (KT)G.g[a][2]};
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-          KT gb[3] = {(KT)G.g[b][0], (KT)G.g[b][1], (KT)G.g[b][2]};
-          KT s = Vm * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+          const KT s = Vm * (ga[0] * gk[b][0] + ga[1] * gk[b][1] + ga[2] * gk[b][2]);
 #pragma unroll
           for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int m = 0; m < 3; ++m)
-              sK.v[warp][lane][9 * b + 3 * k + m] = Vl * ga[k] * gb[m] + Vm * gb[k] * ga[m] + (k == m ? s : (KT)0);
+              sK.v[warp][lane][9 * b + 3 * k + m] =
+                  Vl * ga[k] * gk[b][m] + Vm * gk[b][k] * ga[m] + (k == m ? s : (KT)0);
         }
       } else {
         double Un[4][3];
@@ -145,34 +157,41 @@ tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
         if constexpr (kWantF) {
 #pragma unroll
           for (int i = 0; i < 3; ++i)
-            sF[warp][lane][i] =
-                G.V * (ps.P[i][0] * G.g[a][0] + ps.P[i][1] * G.g[a][1] + ps.P[i][2] * G.g[a][2]);
+            sF[warp][lane][i] = G.V * (ps.P[i][0] * gad[0] + ps.P[i][1] * gad[1] + ps.P[i][2] * gad[2]);
         }
         if constexpr (kWantK) {
           const TangentCoef<KT> tc = tangent_coef<KT>(ps, kappa, G.V);
-          // p_b = F^-T g_b, q_b = F g_b
+          KT Fi[3][3], Fm[3][3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              Fi[i][j] = (KT)ps.Finv[i][j];
+              Fm[i][j] = (KT)ps.F[i][j];
+            }
+          // p_b = F^-T g_b, q_b = F g_b (KT arithmetic)
           KT p[4][3], q[4][3];
 #pragma unroll
           for (int b = 0; b < 4; ++b)
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-              p[b][k] = (KT)(ps.Finv[0][k] * G.g[b][0] + ps.Finv[1][k] * G.g[b][1] + ps.Finv[2][k] * G.g[b][2]);
-              q[b][k] = (KT)(ps.F[k][0] * G.g[b][0] + ps.F[k][1] * G.g[b][1] + ps.F[k][2] * G.g[b][2]);
+              p[b][k] = Fi[0][k] * gk[b][0] + Fi[1][k] * gk[b][1] + Fi[2][k] * gk[b][2];
+              q[b][k] = Fm[k][0] * gk[b][0] + Fm[k][1] * gk[b][1] + Fm[k][2] * gk[b][2];
             }
-          KT pa[3], ha[3], ya[3], ga[3];
+          KT pa[3], ha[3], ya[3];
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
-            pa[k] = p[a][k];
-            ha[k] = tc.hb * p[a][k];
-            ya[k] = tc.c * q[a][k];
-            ga[k] = (KT)G.g[a][k];
+            pa[k] = a == 0 ? p[0][k] : a == 1 ? p[1][k] : a == 2 ? p[2][k] : p[3][k];
+            const KT qa = a == 0 ? q[0][k] : a == 1 ? q[1][k] : a == 2 ? q[2][k] : q[3][k];
+            ha[k] = tc.hb * pa[k];
+            ya[k] = tc.c * qa;
           }
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
             KT wb[3];
 #pragma unroll
             for (int m = 0; m < 3; ++m) wb[m] = tc.A * p[b][m] + tc.c * q[b][m];
-            const KT s = tc.phi * (ga[0] * (KT)G.g[b][0] + ga[1] * (KT)G.g[b][1] + ga[2] * (KT)G.g[b][2]);
+            const KT s = tc.phi * (ga[0] * gk[b][0] + ga[1] * gk[b][1] + ga[2] * gk[b][2]);
 #pragma unroll
             for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -193,10 +212,10 @@ tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
           const int rb = (code >> (2 + 7 * b)) & 127;
           if (rb == lane) {
 #pragma unroll
-            for (int j = 0; j < 9; ++j) acc0[j] += (double)sK.v[warp][t][9 * b + j];
+            for (int j = 0; j < 9; ++j) acc0[j] += sK.v[warp][t][9 * b + j];
           } else if (rb == lane + 32) {
 #pragma unroll
-            for (int j = 0; j < 9; ++j) acc1[j] += (double)sK.v[warp][t][9 * b + j];
+            for (int j = 0; j < 9; ++j) acc1[j] += sK.v[warp][t][9 * b + j];
           }
         }
       }
@@ -218,11 +237,11 @@ tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
       const int64_t row = base + 3 * (int64_t)deg * k;
       if (lane < deg) {
 #pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[row + 3 * lane + m] = (KT)acc0[3 * k + m];
+        for (int m = 0; m < 3; ++m) k_out[row + 3 * lane + m] = acc0[3 * k + m];
       }
       if (lane + 32 < deg) {
 #pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[row + 3 * (lane + 32) + m] = (KT)acc1[3 * k + m];
+        for (int m = 0; m < 3; ++m) k_out[row + 3 * (lane + 32) + m] = acc1[3 * k + m];
       }
     }
   }

@@ -62,8 +62,9 @@ def test_cfg1_seeded_state_fp64():
     assert np.array_equal(K.indptr, g["K_indptr"]) and np.array_equal(K.indices, g["K_indices"])
     assert rel_max(K.data, g["K_data"]) < 1e-13
     assert rel_2(f, g["f"]) < 1e-12
+    # the fused sweep evaluates the same formulas; FMA contraction may differ by an ulp
     f2, K2 = el.assemble_force_and_tangent(m, g["u"])
-    assert np.array_equal(f2, f) and np.array_equal(K2.data, K.data)
+    assert rel_max(f2, f) < 1e-14 and rel_max(K2.data, K.data) < 1e-14
 
 
 def test_cfg1_fp32_mixed_error_bounds():
