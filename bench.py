@@ -294,13 +294,14 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": bytes_mixed, "kernel": "tet4_node_kernel<float,F|K>"},
+                         "algorithmic_bytes_per_launch": bytes_mixed, "kernel": "tet4_fused_kernel<float,F|K> (element records + owner gather)",
+                         "launches_per_step": asm.launches_per_call("fp32-mixed")},
             "fp64": {"value": world * E / (ms_fp64 * 1e-3), "unit": "elements/s", "ms_per_step": ms_fp64,
                      "achieved_gbs": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9,
                      "frac": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9 / peak},
             "mixed_over_fp64": ms_fp64 / ms_mixed,
             "accuracy": {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err},
-            "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps,
+            "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps * asm.launches_per_call("fp32-mixed"),
             "clocks": clk,
         }
         print(json.dumps(line))

@@ -50,9 +50,6 @@ extern "C" {
 #define PSX_FP64 0              /* everything in FP64, K values stored as double */
 #define PSX_FP32_MIXED 1        /* f_int, det F and ln J in FP64; K_T in FP32, stored as float */
 
-/* Largest node degree (distinct neighbours incl. itself) psx_tet4_assemble accepts. */
-#define PSX_TET4_MAX_DEGREE 64
-
 /*
  * Status block written by the element kernels (device memory, psx_status_bytes()
  * bytes, zero it before a call).  Layout: int32 n_inverted, int32 n_bad_volume,
@@ -108,28 +105,76 @@ int psx_block_lists(const int64_t* conn, int64_t E, int npe, int64_t N,
                     const int32_t* nbr_ptr, const int32_t* nbr,
                     int32_t* blk_ptr, int32_t* blk_src);
 
+/* ---- Gather plan (host, once per mesh) ------------------------------------- */
+
+/*
+ * Plan of the element-record / owner-gather assembly.  Items are the node pairs
+ * (i < j) of the node graph and the nodes; every item lists the element slots that
+ * contribute to it (ascending element order) and the items are sorted by the last
+ * element they need, so the items completed by element chunk k can be gathered right
+ * after chunk k has been evaluated.  Pointers marked device/host as noted.
+ */
+typedef struct psx_plan {
+  int32_t npe;              /* nodes per element: 4 or 10 */
+  int32_t n_granules;       /* ceil(n_elements / granule) */
+  int64_t n_elements;
+  int64_t n_nodes;
+  int64_t n_pairs;          /* node pairs i < j */
+  int64_t granule;          /* plan resolution in elements (power of two) */
+  int64_t max_span;         /* max over items of (last - first contributing element) */
+  const int32_t* conn;      /* device, E x npe int32 */
+  const int32_t* pair_info; /* device, 4 per pair: pos_up, stride_up, pos_lo, stride_lo */
+  const int32_t* pair_ptr;  /* device, n_pairs + 1 */
+  const int32_t* pair_src;  /* device, e * 64 + local pair slot */
+  const int32_t* node_info; /* device, 4 per node item: pos_diag, stride, node, 0 */
+  const int32_t* node_ptr;  /* device, N + 1 */
+  const int32_t* node_src;  /* device, e * 16 + local node index */
+  const int32_t* pair_gptr; /* host, n_granules + 1: pair items ready in each granule */
+  const int32_t* node_gptr; /* host, n_granules + 1 */
+} psx_plan_t;
+
+/* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */
+int psx_plan_count(const int64_t* conn, int64_t E, int npe, int64_t N, const int32_t* nbr_ptr,
+                   int64_t* n_pairs, int64_t* n_pair_src);
+
+/*
+ * Fill the plan arrays (host memory; the caller uploads the device ones):
+ * pair_info (4 n_pairs), pair_ptr (n_pairs+1), pair_src (E npe (npe-1)/2),
+ * pair_gptr (n_granules+1), node_info (4 N), node_ptr (N+1), node_src (E npe),
+ * node_gptr (n_granules+1), max_span (1).  PSX_ERR_LIMIT if E > 2^25.
+ */
+int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int32_t* nbr_ptr,
+                  const int32_t* nbr, int64_t granule, int32_t* pair_info, int32_t* pair_ptr,
+                  int32_t* pair_src, int32_t* pair_gptr, int32_t* node_info, int32_t* node_ptr,
+                  int32_t* node_src, int32_t* node_gptr, int64_t* max_span);
+
+/*
+ * Workspace the assembly needs for chunks of `chunk_elems` elements (a multiple of
+ * the plan granule): a ring of element records, *ring_elems records long.
+ */
+int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t chunk_elems, int64_t* ring_elems,
+                   int64_t* bytes);
+
 /* ---- Tet4 element kernels (device) ----------------------------------------- */
 
 /*
  * Tet4 Total-Lagrangian NeoHookean assembly (replaces the element loops of
- * domain/solid.py:230-325 and the COO->CSR / np.add.at scatter).
- *   conn (device, E x 4 int32), X, u (device, N x 3 double; u ignored for PSX_LINEAR)
+ * domain/solid.py:172-207, 230-325 and the COO->CSR / np.add.at scatter).
+ *   X, u (device, N x 3 double; u ignored for PSX_LINEAR)
  *   mu_e, kappa_e (device, E doubles) per-element moduli, or NULL to use mu, kappa
  *   lam: Lame lambda for PSX_LINEAR (with mu)
- *   graph arrays from psx_graph_fill (device copies), max_degree = max node degree
  *   f_out (device, 3N doubles) when mode has PSX_WANT_F
- *   k_out (device, nnz values: double for PSX_FP64, float for PSX_FP32_MIXED)
+ *   k_out (device, nnz values in psx_csr_pattern order: double for PSX_FP64, float
+ *          for PSX_FP32_MIXED) when mode has PSX_WANT_K or PSX_LINEAR
+ *   work (device, >= psx_work_bytes, 256-byte aligned) scratch ring of element records
  *   status (device, psx_status_bytes(), zeroed by the caller)
  * Deterministic: every output value is a fixed-order sum; no atomics touch f or K.
  */
-int psx_tet4_assemble(const int32_t* conn, const double* X, const double* u,
-                      const double* mu_e, const double* kappa_e,
-                      double mu, double kappa, double lam,
-                      int64_t E, int64_t N,
-                      const int32_t* nbr_ptr, const int32_t* inc_ptr,
-                      const int32_t* inc_elem, const uint32_t* inc_code, int max_degree,
-                      int mode, int precision,
-                      double* f_out, void* k_out, void* status, void* stream);
+int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u,
+                      const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,
+                      int mode, int precision, int64_t chunk_elems,
+                      double* f_out, void* k_out, void* work, int64_t work_bytes,
+                      void* status, void* stream);
 
 /*
  * Reference det (of [1 X], = 6 V) and det F of one element, written to out2

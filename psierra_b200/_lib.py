@@ -23,8 +23,6 @@ PSX_LINEAR = 4
 PSX_FP64 = 0
 PSX_FP32_MIXED = 1
 
-PSX_TET4_MAX_DEGREE = 64
-
 _ERRORS = {
     PSX_ERR_ARG: "invalid argument",
     PSX_ERR_CUDA: "CUDA launch or copy failed",
@@ -42,10 +40,37 @@ SIGNATURES: dict[str, list] = {
     "psx_graph_fill": [_p, _i64, _i32, _i64, _p, _p, _p, _p, _p],
     "psx_csr_pattern": [_i64, _p, _p, _p, _p],
     "psx_block_lists": [_p, _i64, _i32, _i64, _p, _p, _p, _p],
-    "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i64, _i64, _p, _p, _p, _p, _i32,
-                          _i32, _i32, _p, _p, _p, _p],
+    "psx_plan_count": [_p, _i64, _i32, _i64, _p, _p, _p],
+    "psx_plan_fill": [_p, _i64, _i32, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _p, _p, _p],
+    "psx_work_bytes": [_p, _i32, _i64, _p, _p],
+    "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _i64, _p, _p, _p, _i64, _p, _p],
     "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
 }
+
+
+
+class PlanStruct(ctypes.Structure):
+    """Mirror of ``psx_plan_t`` (include/psierra_b200.h)."""
+
+    _fields_ = [
+        ("npe", ctypes.c_int32),
+        ("n_granules", ctypes.c_int32),
+        ("n_elements", ctypes.c_int64),
+        ("n_nodes", ctypes.c_int64),
+        ("n_pairs", ctypes.c_int64),
+        ("granule", ctypes.c_int64),
+        ("max_span", ctypes.c_int64),
+        ("conn", ctypes.c_void_p),
+        ("pair_info", ctypes.c_void_p),
+        ("pair_ptr", ctypes.c_void_p),
+        ("pair_src", ctypes.c_void_p),
+        ("node_info", ctypes.c_void_p),
+        ("node_ptr", ctypes.c_void_p),
+        ("node_src", ctypes.c_void_p),
+        ("pair_gptr", ctypes.c_void_p),
+        ("node_gptr", ctypes.c_void_p),
+    ]
+
 
 _lib: ctypes.CDLL | None = None
 

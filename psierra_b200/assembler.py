@@ -15,6 +15,8 @@ as the reference's element loop would.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -52,6 +54,8 @@ class GPUAssembler:
         nbytes = int(lib().psx_status_bytes())
         self.status = torch.zeros((nbytes + 3) // 4, dtype=torch.int32, device=self.device)
         self._dets = torch.zeros(2, dtype=torch.float64, device=self.device)
+        self._work: dict = {}
+        self.chunk_elems = self.default_chunk(precision)
         self.set_material(material)
 
     # ------------------------------------------------------------------ material
@@ -86,6 +90,31 @@ class GPUAssembler:
     def new_k(self, precision: str | None = None) -> torch.Tensor:
         return torch.empty(self.nnz, dtype=self.k_dtype(precision), device=self.device)
 
+    # ------------------------------------------------------------------ workspace
+    def default_chunk(self, precision: str) -> int:
+        """Elements per launch: keeps the ring of element records well inside L2."""
+        g = self.pattern.GRANULE
+        c = 32768 if precision == "fp32-mixed" else 16384
+        return max(g, (min(c, self.n_elements + g - 1) // g) * g)
+
+    def launches_per_call(self, precision: str | None = None) -> int:
+        """Kernel launches one assemble() call makes (one per element chunk, plus one)."""
+        prec = precision or self.precision
+        chunk = self.chunk_elems if prec == self.precision else self.default_chunk(prec)
+        return (self.n_elements + chunk - 1) // chunk + 1
+
+    def workspace(self, precision: str, chunk: int) -> torch.Tensor:
+        key = (precision, chunk)
+        w = self._work.get(key)
+        if w is None:
+            ring = ctypes.c_int64()
+            nbytes = ctypes.c_int64()
+            check(lib().psx_work_bytes(ctypes.byref(self.dev["plan"]), PRECISIONS[precision], chunk,
+                                       ctypes.byref(ring), ctypes.byref(nbytes)), "psx_work_bytes")
+            w = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+            self._work = {key: w}  # keep one workspace alive
+        return w
+
     # ------------------------------------------------------------------ kernels
     def assemble(self, u: torch.Tensor | None, want_f: bool = True, want_k: bool = True,
                  precision: str | None = None, f_out: torch.Tensor | None = None,
@@ -118,14 +147,13 @@ class GPUAssembler:
         if want_k and k_out.dtype != self.k_dtype(prec):
             raise ValueError(f"k_out must be {self.k_dtype(prec)} for precision {prec}")
         self.status.zero_()
-        d = self.dev
+        chunk = self.chunk_elems if prec == self.precision else self.default_chunk(prec)
+        work = self.workspace(prec, chunk)
         rc = lib().psx_tet4_assemble(
-            ptr(d["conn"]), ptr(self.X), ptr(u) if not linear else None,
-            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam,
-            self.n_elements, self.n_nodes, ptr(d["nbr_ptr"]), ptr(d["inc_ptr"]), ptr(d["inc_elem"]),
-            ptr(d["inc_code"]), self.pattern.max_degree, mode, PRECISIONS[prec],
-            ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(self.status),
-            _stream_handle())
+            ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u) if not linear else None,
+            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam, mode, PRECISIONS[prec], chunk,
+            ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(work), work.numel(),
+            ptr(self.status), _stream_handle())
         check(rc, "psx_tet4_assemble")
         if check_status:
             self.raise_on_bad_elements(u)

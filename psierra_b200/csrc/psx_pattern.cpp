@@ -158,3 +158,158 @@ extern "C" int psx_block_lists(const int64_t* conn, int64_t E, int npe, int64_t 
     }
   return PSX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Gather plan for the element-record / owner-gather assembly.
+//
+// Items: every node pair (i < j) of the node graph ("pair", off-diagonal block K_ij and
+// its transpose K_ji) and every node ("node", diagonal block K_ii and f_i).  Each item
+// lists its contributing element slots in ascending element order; items are sorted by
+// their "ready" element (the largest contributing element id), so that the items
+// completed by an element range [0, c) form a prefix, and granule ranges of the sorted
+// item lists can be gathered right after that element range has been evaluated.
+namespace {
+
+inline int local_pair_index(int a, int b, int npe) {  // a < b
+  return a * npe - a * (a + 1) / 2 + (b - a - 1);
+}
+
+struct Item {
+  int32_t ready;
+  int32_t order;  // tie break: original item index
+};
+
+}  // namespace
+
+extern "C" int psx_plan_count(const int64_t* conn, int64_t E, int npe, int64_t N, const int32_t* nbr_ptr,
+                              int64_t* n_pairs, int64_t* n_pair_src) {
+  if (!args_ok(conn, E, npe, N) || !nbr_ptr || !n_pairs || !n_pair_src) return PSX_ERR_ARG;
+  if (E > ((int64_t)1 << 25)) return PSX_ERR_LIMIT;  // slot encoding e * 64 + slot must fit int32
+  *n_pairs = ((int64_t)nbr_ptr[N] - N) / 2;
+  *n_pair_src = E * (int64_t)(npe * (npe - 1) / 2);
+  return PSX_OK;
+}
+
+extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int32_t* nbr_ptr,
+                             const int32_t* nbr, int64_t granule, int32_t* pair_info, int32_t* pair_ptr,
+                             int32_t* pair_src, int32_t* pair_gptr, int32_t* node_info, int32_t* node_ptr,
+                             int32_t* node_src, int32_t* node_gptr, int64_t* max_span) {
+  if (!args_ok(conn, E, npe, N) || !nbr_ptr || !nbr || granule <= 0 || !pair_info || !pair_ptr || !pair_src ||
+      !pair_gptr || !node_info || !node_ptr || !node_src || !node_gptr || !max_span)
+    return PSX_ERR_ARG;
+  if (E > ((int64_t)1 << 25)) return PSX_ERR_LIMIT;
+  std::vector<int32_t> ptr, elem;
+  std::vector<int8_t> local;
+  incidences(conn, E, npe, N, ptr, elem, local);
+  const int64_t n_pairs = ((int64_t)nbr_ptr[N] - N) / 2;
+  const int64_t n_gran = (E + granule - 1) / granule;
+
+  // ---- pairs in (i, j) order: contributions = inc(i) intersect inc(j)
+  std::vector<int32_t> p_ptr(n_pairs + 1, 0), p_src;
+  std::vector<int32_t> p_info(4 * n_pairs);
+  std::vector<Item> p_item(n_pairs);
+  std::vector<int32_t> p_min(n_pairs);
+  p_src.reserve((size_t)E * (npe * (npe - 1) / 2));
+  int64_t p = 0;
+  for (int64_t i = 0; i < N; ++i) {
+    const int32_t b0 = nbr_ptr[i], deg = nbr_ptr[i + 1] - b0;
+    for (int32_t r = 0; r < deg; ++r) {
+      const int64_t j = nbr[b0 + r];
+      if (j <= i) continue;
+      const int32_t* ej = nbr + nbr_ptr[j];
+      const int32_t degj = nbr_ptr[j + 1] - nbr_ptr[j];
+      const int32_t rji = (int32_t)(std::lower_bound(ej, ej + degj, (int32_t)i) - ej);
+      p_info[4 * p + 0] = 9 * b0 + 3 * r;
+      p_info[4 * p + 1] = 3 * deg;
+      p_info[4 * p + 2] = 9 * nbr_ptr[j] + 3 * rji;
+      p_info[4 * p + 3] = 3 * degj;
+      int32_t si = ptr[i], sj = ptr[j], emax = -1, emin = 0x7fffffff;
+      while (si < ptr[i + 1] && sj < ptr[j + 1]) {
+        if (elem[si] < elem[sj]) {
+          ++si;
+        } else if (elem[si] > elem[sj]) {
+          ++sj;
+        } else {
+          const int a = local[si], b = local[sj];
+          const int slot = local_pair_index(std::min(a, b), std::max(a, b), npe);
+          p_src.push_back(elem[si] * 64 + slot);
+          emax = std::max(emax, elem[si]);
+          emin = std::min(emin, elem[si]);
+          ++si;
+          ++sj;
+        }
+      }
+      if (emax < 0) return PSX_ERR_ARG;  // a graph edge must come from some element
+      p_ptr[p + 1] = (int32_t)p_src.size();
+      p_item[p] = {emax, (int32_t)p};
+      p_min[p] = emin;
+      ++p;
+    }
+  }
+  if (p != n_pairs) return PSX_ERR_ARG;
+
+  // ---- nodes: contributions = inc(i)
+  std::vector<Item> n_item(N);
+  int64_t span = 0;
+  for (int64_t i = 0; i < N; ++i) {
+    if (ptr[i + 1] == ptr[i]) {
+      n_item[i] = {-1, (int32_t)i};  // isolated node: ready before everything
+      continue;
+    }
+    const int32_t emin = elem[ptr[i]], emax = elem[ptr[i + 1] - 1];
+    n_item[i] = {emax, (int32_t)i};
+    span = std::max<int64_t>(span, emax - emin);
+  }
+  for (int64_t q = 0; q < n_pairs; ++q) span = std::max<int64_t>(span, p_item[q].ready - p_min[q]);
+  *max_span = span;
+
+  auto by_ready = [](const Item& x, const Item& y) {
+    return x.ready < y.ready || (x.ready == y.ready && x.order < y.order);
+  };
+  std::sort(p_item.begin(), p_item.end(), by_ready);
+  std::sort(n_item.begin(), n_item.end(), by_ready);
+
+  // ---- emit pairs in ready order
+  int32_t out = 0;
+  pair_ptr[0] = 0;
+  for (int64_t k = 0; k < n_pairs; ++k) {
+    const int32_t q = p_item[k].order;
+    std::memcpy(pair_info + 4 * k, p_info.data() + 4 * q, 4 * sizeof(int32_t));
+    for (int32_t s = p_ptr[q]; s < p_ptr[q + 1]; ++s) pair_src[out++] = p_src[s];
+    pair_ptr[k + 1] = out;
+  }
+  // granule ranges: items whose ready element lies in granule g
+  {
+    int64_t k = 0;
+    for (int64_t g = 0; g <= n_gran; ++g) {
+      const int64_t limit = std::min<int64_t>(E, g * granule);  // ready < limit
+      while (k < n_pairs && p_item[k].ready < limit) ++k;
+      pair_gptr[g] = (int32_t)k;
+    }
+    pair_gptr[n_gran] = (int32_t)n_pairs;
+  }
+  // ---- emit nodes in ready order
+  out = 0;
+  node_ptr[0] = 0;
+  for (int64_t k = 0; k < N; ++k) {
+    const int32_t i = n_item[k].order;
+    const int32_t b0 = nbr_ptr[i], deg = nbr_ptr[i + 1] - b0;
+    const int32_t rii = (int32_t)(std::lower_bound(nbr + b0, nbr + b0 + deg, i) - (nbr + b0));
+    node_info[4 * k + 0] = 9 * b0 + 3 * rii;
+    node_info[4 * k + 1] = 3 * deg;
+    node_info[4 * k + 2] = i;
+    node_info[4 * k + 3] = 0;
+    for (int32_t s = ptr[i]; s < ptr[i + 1]; ++s) node_src[out++] = elem[s] * 16 + local[s];
+    node_ptr[k + 1] = out;
+  }
+  {
+    int64_t k = 0;
+    for (int64_t g = 0; g <= n_gran; ++g) {
+      const int64_t limit = std::min<int64_t>(E, g * granule);
+      while (k < N && n_item[k].ready < limit) ++k;
+      node_gptr[g] = (int32_t)k;
+    }
+    node_gptr[n_gran] = (int32_t)N;
+  }
+  return PSX_OK;
+}

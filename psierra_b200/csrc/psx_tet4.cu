@@ -5,23 +5,29 @@
 // (element/tet4_total_lagrangian.py:77-139) and the COO->CSR / np.add.at scatter
 // (utility/assembly.py:37-108).
 //
-// Owner-computes layout: one warp owns one node i and writes its three CSR rows and
-// its three f entries exactly once.  Lane t of the warp evaluates incidence t of the
-// node (element e holding i at local index a): the blocks K_ab (b = 0..3) and f_a.
-// The blocks are staged in shared memory and lane r then sums, in ascending element
-// order, every staged block whose neighbour rank is r.  Each output value is a
-// fixed-order sum, so results are bitwise reproducible run to run; no atomics touch
-// f or K.  Writes of a row are contiguous across lanes (lane r writes columns
-// 3r..3r+2 of each of the three rows).
+// Two phases per element chunk, fused into one launch per chunk:
+//   A (element-centric): one thread per element evaluates the kinematics, the NeoHookean
+//     stress and tangent, its 10 distinct 3x3 tangent blocks and its 4 nodal force
+//     vectors, once, and writes them to an L2-resident ring of element records
+//     (psx_gather.cuh).
+//   B (owner-computes gather): one thread per node pair / node sums the records of the
+//     elements that share it, in ascending element order, and writes each CSR value and
+//     each f entry exactly once.
+// Launch k runs A on element chunk k and B on the items completed by chunk k-1, so the
+// two overlap and the ring only ever holds a few chunks.  No atomics touch f or K, so
+// results are bitwise reproducible run to run.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "psx_common.cuh"
+#include "psx_gather.cuh"
 
 namespace psx {
 namespace {
 
-constexpr int kWarps = 4;  // warps (nodes) per block
+constexpr int kThreads = 128;
 
 struct Tet4Geom {
   double g[4][3];  // shape-function gradients
@@ -72,186 +78,149 @@ __device__ __forceinline__ void tet4_grad(const double Un[4][3], const Tet4Geom&
     }
 }
 
-template <typename KT>
-struct KStage {
-  KT v[kWarps][32][37];  // 4 blocks x 9 values, padded
+struct Tet4Args {
+  const int32_t* conn;
+  const double* X;
+  const double* U;
+  const double* mu_e;
+  const double* kappa_e;
+  double mu0, kappa0, lam0;
+  Status* st;
 };
 
+// Phase A: one element -> its record.  tet4_total_lagrangian.py:77-139 (and, with
+// PSX_LINEAR, tet4_base.py:129-136) in the closed form of psx_common.cuh.
 template <typename KT, int MODE>
-__global__ void __launch_bounds__(kWarps * 32)
-tet4_node_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X, const double* __restrict__ U,
-                 const double* __restrict__ mu_e, const double* __restrict__ kappa_e, double mu0,
-                 double kappa0, double lam0, int32_t N, const int32_t* __restrict__ nbr_ptr,
-                 const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc_elem,
-                 const uint32_t* __restrict__ inc_code, double* __restrict__ f_out, KT* __restrict__ k_out,
-                 Status* __restrict__ st) {
+__device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
+                                             double* __restrict__ frec) {
+  using L = RecLayout<4>;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
-  __shared__ KStage<KT> sK;
-  __shared__ double sF[kWarps][32][3];
-  __shared__ uint32_t sCode[kWarps][32];
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int node = blockIdx.x * kWarps + warp;
-  if (node >= N) return;  // uniform per warp
-  const int i0 = inc_ptr[node], i1 = inc_ptr[node + 1];
-  const int nb0 = nbr_ptr[node], deg = nbr_ptr[node + 1] - nb0;
-
-  KT acc0[9], acc1[9];
-  double facc[3];
+  constexpr bool kWantK = (MODE & PSX_WANT_K) != 0 || kLinear;
+  const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
+  double Xn[4][3];
+  load_nodes(A.X, cn, Xn);
+  Tet4Geom G;
+  tet4_geometry(Xn, G);
+  if (!(G.detD > 0.0)) flag_bad_element(A.st, e, true);
+  KT p[4][3], q[4][3];
+  TangentCoef<KT> tc;
+  KT gk[4][3];
 #pragma unroll
-  for (int j = 0; j < 9; ++j) acc0[j] = acc1[j] = (KT)0;
-  facc[0] = facc[1] = facc[2] = 0.0;
-
-  for (int c0 = i0; c0 < i1; c0 += 32) {
-    const int cnt = min(32, i1 - c0);
-    if (lane < cnt) {
-      const int s = c0 + lane;
-      const int e = inc_elem[s];
-      const uint32_t code = inc_code[s];
-      const int a = code & 3;
-      const int4 cn = __ldg(reinterpret_cast<const int4*>(conn) + e);
-      double Xn[4][3];
-      load_nodes(X, cn, Xn);
-      Tet4Geom G;
-      tet4_geometry(Xn, G);
-      const double mu = mu_e ? mu_e[e] : mu0;
-      const double kappa = kappa_e ? kappa_e[e] : kappa0;
-      if (a == 0 && !(G.detD > 0.0)) flag_bad_element(st, e, true);
-      sCode[warp][lane] = code;
-
-      // Own-node vectors are picked with selects so nothing is indexed at run time.
-      double gad[3];
+  for (int b = 0; b < 4; ++b)
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
-        gad[k] = a == 0 ? G.g[0][k] : a == 1 ? G.g[1][k] : a == 2 ? G.g[2][k] : G.g[3][k];
-      KT gk[4][3];
+    for (int k = 0; k < 3; ++k) gk[b][k] = (KT)G.g[b][k];
+  if constexpr (kLinear) {
+    // small-strain: p = q = g, K_ab = V [lam g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I]
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) p[b][k] = q[b][k] = gk[b][k];
+    tc.A = (KT)(G.V * A.lam0);
+    tc.hb = (KT)(G.V * A.mu0);
+    tc.c = (KT)0;
+    tc.phi = (KT)(G.V * A.mu0);
+  } else {
+    const double mu = A.mu_e ? A.mu_e[e] : A.mu0;
+    const double kappa = A.kappa_e ? A.kappa_e[e] : A.kappa0;
+    double Un[4][3], l[3][3];
+    load_nodes(A.U, cn, Un);
+    tet4_grad(Un, G, l);
+    PointState ps;
+    neohookean_point(l, mu, kappa, ps);
+    if (G.detD > 0.0 && ps.Jm1 <= -1.0) flag_bad_element(A.st, e, false);
+    if constexpr (kWantF) {
+      double fr[12];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+          fr[3 * a + i] = G.V * (ps.P[i][0] * G.g[a][0] + ps.P[i][1] * G.g[a][1] + ps.P[i][2] * G.g[a][2]);
+      double2* fq = reinterpret_cast<double2*>(frec);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(fr[2 * i], fr[2 * i + 1]));
+    }
+    if constexpr (kWantK) {
+      tc = tangent_coef<KT>(ps, kappa, G.V);
+      KT Fi[3][3], Fm[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          Fi[i][j] = (KT)ps.Finv[i][j];
+          Fm[i][j] = (KT)ps.F[i][j];
+        }
 #pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) gk[b][k] = (KT)G.g[b][k];
-      const KT ga[3] = {(KT)gad[0], (KT)gad[1], (KT)gad[2]};
-
-      if constexpr (kLinear) {
-        // tet4_base.py:129-136: K_ab = V [lam g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I]
-        const KT Vl = (KT)(G.V * lam0), Vm = (KT)(G.V * mu0);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const KT s = Vm * (ga[0] * gk[b][0] + ga[1] * gk[b][1] + ga[2] * gk[b][2]);
-#pragma unroll
-          for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-              sK.v[warp][lane][9 * b + 3 * k + m] =
-                  Vl * ga[k] * gk[b][m] + Vm * gk[b][k] * ga[m] + (k == m ? s : (KT)0);
+        for (int k = 0; k < 3; ++k) {
+          p[b][k] = Fi[0][k] * gk[b][0] + Fi[1][k] * gk[b][1] + Fi[2][k] * gk[b][2];
+          q[b][k] = Fm[k][0] * gk[b][0] + Fm[k][1] * gk[b][1] + Fm[k][2] * gk[b][2];
         }
-      } else {
-        double Un[4][3];
-        load_nodes(U, cn, Un);
-        double l[3][3];
-        tet4_grad(Un, G, l);
-        PointState ps;
-        neohookean_point(l, mu, kappa, ps);
-        if (a == 0 && G.detD > 0.0 && ps.Jm1 <= -1.0) flag_bad_element(st, e, false);
-        if constexpr (kWantF) {
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-            sF[warp][lane][i] = G.V * (ps.P[i][0] * gad[0] + ps.P[i][1] * gad[1] + ps.P[i][2] * gad[2]);
-        }
-        if constexpr (kWantK) {
-          const TangentCoef<KT> tc = tangent_coef<KT>(ps, kappa, G.V);
-          KT Fi[3][3], Fm[3][3];
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              Fi[i][j] = (KT)ps.Finv[i][j];
-              Fm[i][j] = (KT)ps.F[i][j];
-            }
-          // p_b = F^-T g_b, q_b = F g_b (KT arithmetic)
-          KT p[4][3], q[4][3];
-#pragma unroll
-          for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              p[b][k] = Fi[0][k] * gk[b][0] + Fi[1][k] * gk[b][1] + Fi[2][k] * gk[b][2];
-              q[b][k] = Fm[k][0] * gk[b][0] + Fm[k][1] * gk[b][1] + Fm[k][2] * gk[b][2];
-            }
-          KT pa[3], ha[3], ya[3];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            pa[k] = a == 0 ? p[0][k] : a == 1 ? p[1][k] : a == 2 ? p[2][k] : p[3][k];
-            const KT qa = a == 0 ? q[0][k] : a == 1 ? q[1][k] : a == 2 ? q[2][k] : q[3][k];
-            ha[k] = tc.hb * pa[k];
-            ya[k] = tc.c * qa;
-          }
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            KT wb[3];
-#pragma unroll
-            for (int m = 0; m < 3; ++m) wb[m] = tc.A * p[b][m] + tc.c * q[b][m];
-            const KT s = tc.phi * (ga[0] * gk[b][0] + ga[1] * gk[b][1] + ga[2] * gk[b][2]);
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-              for (int m = 0; m < 3; ++m)
-                sK.v[warp][lane][9 * b + 3 * k + m] =
-                    pa[k] * wb[m] + p[b][k] * ha[m] + ya[k] * p[b][m] + (k == m ? s : (KT)0);
-          }
-        }
-      }
     }
-    __syncwarp();
-    // Fixed-order reduction: lane r owns neighbour columns r and r + 32.
-    for (int t = 0; t < cnt; ++t) {
-      const uint32_t code = sCode[warp][t];
-      if constexpr (kWantK) {
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int rb = (code >> (2 + 7 * b)) & 127;
-          if (rb == lane) {
-#pragma unroll
-            for (int j = 0; j < 9; ++j) acc0[j] += sK.v[warp][t][9 * b + j];
-          } else if (rb == lane + 32) {
-#pragma unroll
-            for (int j = 0; j < 9; ++j) acc1[j] += sK.v[warp][t][9 * b + j];
-          }
-        }
-      }
-      if constexpr (kWantF && !kLinear) {
-        if (lane == 0) {
-          facc[0] += sF[warp][t][0];
-          facc[1] += sF[warp][t][1];
-          facc[2] += sF[warp][t][2];
-        }
-      }
-    }
-    __syncwarp();
   }
-
   if constexpr (kWantK) {
-    const int64_t base = 9 * (int64_t)nb0;
+    // K_ab[k][m] = p_a,k w_b,m + p_b,k h_a,m + y_a,k p_b,m + s_ab d_km
+    KT w[4][3], h[4][3], y[4][3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int64_t row = base + 3 * (int64_t)deg * k;
-      if (lane < deg) {
+    for (int b = 0; b < 4; ++b)
 #pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[row + 3 * lane + m] = acc0[3 * k + m];
+      for (int k = 0; k < 3; ++k) {
+        w[b][k] = tc.A * p[b][k] + tc.c * q[b][k];
+        h[b][k] = tc.hb * p[b][k];
+        y[b][k] = tc.c * q[b][k];
       }
-      if (lane + 32 < deg) {
+    const int gid[4] = {cn.x, cn.y, cn.z, cn.w};
+    int slot = 0;
 #pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[row + 3 * (lane + 32) + m] = acc1[3 * k + m];
+    for (int a = 0; a < 4; ++a) {
+#pragma unroll
+      for (int b = a; b < 4; ++b) {
+        const KT s = tc.phi * (gk[a][0] * gk[b][0] + gk[a][1] * gk[b][1] + gk[a][2] * gk[b][2]);
+        KT v[9];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+            v[3 * k + m] = p[a][k] * w[b][m] + p[b][k] * h[a][m] + y[a][k] * p[b][m] + (k == m ? s : (KT)0);
+        if (b == a) {
+          const KT d[6] = {v[0], v[1], v[2], v[4], v[5], v[8]};
+          store_diag_block<KT>(krec + L::diag_off(a), d);
+        } else {
+          store_pair_block<KT>(krec + L::pair_off(slot), v, gid[a] > gid[b]);
+          ++slot;
+        }
       }
     }
   }
-  if constexpr (kWantF && !kLinear) {
-    if (lane == 0) {
-      f_out[3 * (int64_t)node + 0] = facc[0];
-      f_out[3 * (int64_t)node + 1] = facc[1];
-      f_out[3 * (int64_t)node + 2] = facc[2];
+}
+
+template <typename KT, int MODE>
+__global__ void __launch_bounds__(kThreads, 4)
+tet4_fused_kernel(Tet4Args A, GatherArgs g, int64_t e0, int64_t e1, int32_t nA, int32_t nP,
+                  KT* __restrict__ krec, double* __restrict__ frec, KT* __restrict__ k_out,
+                  double* __restrict__ f_out) {
+  using L = RecLayout<4>;
+  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+  int32_t b = blockIdx.x;
+  if (b < nA) {
+    const int64_t e = e0 + (int64_t)b * kThreads + threadIdx.x;
+    if (e < e1) {
+      const int64_t slot = e & g.ring_mask;
+      tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
     }
+    return;
   }
+  b -= nA;
+  if (b < nP) {
+    const int32_t p = g.p0 + b * kThreads + threadIdx.x;
+    if (p < g.p1) gather_pair<KT, 4>(g, p, krec, k_out);
+    return;
+  }
+  b -= nP;
+  const int32_t n = g.n0 + b * kThreads + threadIdx.x;
+  if (n < g.n1) gather_node<KT, 4, kWantK, kWantF>(g, n, krec, frec, k_out, f_out);
 }
 
 __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
@@ -276,42 +245,118 @@ __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double*
 }
 
 template <typename KT, int MODE>
-int launch_tet4(const int32_t* conn, const double* X, const double* u, const double* mu_e,
-                const double* kappa_e, double mu, double kappa, double lam, int64_t N, const int32_t* nbr_ptr,
-                const int32_t* inc_ptr, const int32_t* inc_elem, const uint32_t* inc_code, double* f_out,
-                void* k_out, void* status, cudaStream_t stream) {
-  const unsigned blocks = (unsigned)((N + kWarps - 1) / kWarps);
-  tet4_node_kernel<KT, MODE><<<blocks, kWarps * 32, 0, stream>>>(
-      conn, X, u, mu_e, kappa_e, mu, kappa, lam, (int32_t)N, nbr_ptr, inc_ptr, inc_elem, inc_code, f_out,
-      static_cast<KT*>(k_out), static_cast<Status*>(status));
-  PSX_CUDA_CHECK_LAUNCH();
+int run_tet4(const psx_plan_t* P, const Tet4Args& A, int64_t chunk, int64_t ring, KT* krec, double* frec,
+             KT* k_out, double* f_out, cudaStream_t stream) {
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+  const int64_t E = P->n_elements;
+  const int64_t G = chunk / P->granule;  // granules per chunk
+  const int64_t n_chunks = (E + chunk - 1) / chunk;
+  GatherArgs g;
+  g.pair_info = P->pair_info;
+  g.pair_ptr = P->pair_ptr;
+  g.pair_src = P->pair_src;
+  g.node_info = P->node_info;
+  g.node_ptr = P->node_ptr;
+  g.node_src = P->node_src;
+  g.ring_mask = ring - 1;
+  for (int64_t k = 0; k <= n_chunks; ++k) {
+    int64_t e0 = 0, e1 = 0;
+    int32_t nA = 0, nP = 0, nN = 0;
+    if (k < n_chunks) {
+      e0 = k * chunk;
+      e1 = std::min<int64_t>(E, e0 + chunk);
+      nA = (int32_t)((e1 - e0 + kThreads - 1) / kThreads);
+    }
+    g.p0 = g.p1 = g.n0 = g.n1 = 0;
+    if (k >= 1) {
+      const int64_t ga = (k - 1) * G, gb = std::min<int64_t>(k * G, P->n_granules);
+      if (kWantK) {
+        g.p0 = P->pair_gptr[ga];
+        g.p1 = P->pair_gptr[gb];
+        nP = (g.p1 - g.p0 + kThreads - 1) / kThreads;
+      }
+      g.n0 = (k == 1) ? 0 : P->node_gptr[ga];
+      g.n1 = P->node_gptr[gb];
+      nN = (g.n1 - g.n0 + kThreads - 1) / kThreads;
+    }
+    const int32_t blocks = nA + nP + nN;
+    if (blocks == 0) continue;
+    tet4_fused_kernel<KT, MODE><<<blocks, kThreads, 0, stream>>>(A, g, e0, e1, nA, nP, krec, frec, k_out, f_out);
+    PSX_CUDA_CHECK_LAUNCH();
+  }
   return PSX_OK;
 }
 
 }  // namespace
 }  // namespace psx
 
+namespace {
+
+// Ring of element records: a power of two covering the chunk being written, the
+// chunk being gathered and the item span behind it.
+int64_t ring_elems_for(const psx_plan_t* P, int64_t chunk) {
+  const int64_t need = (P->max_span + chunk - 1) / chunk + 2;
+  int64_t ring = 1;
+  while (ring < need * chunk) ring <<= 1;
+  const int64_t full = [&] {
+    int64_t r = 1;
+    while (r < P->n_elements) r <<= 1;
+    return r;
+  }();
+  return std::min(ring, full);
+}
+
+bool plan_ok(const psx_plan_t* P) {
+  return P && P->conn && P->pair_info && P->pair_ptr && P->pair_src && P->node_info && P->node_ptr &&
+         P->node_src && P->pair_gptr && P->node_gptr && P->n_elements > 0 && P->n_nodes > 0 && P->granule > 0 &&
+         (P->granule & (P->granule - 1)) == 0;
+}
+
+}  // namespace
+
 extern "C" size_t psx_status_bytes(void) { return sizeof(psx::Status); }
 
-extern "C" int psx_tet4_assemble(const int32_t* conn, const double* X, const double* u, const double* mu_e,
-                                 const double* kappa_e, double mu, double kappa, double lam, int64_t E,
-                                 int64_t N, const int32_t* nbr_ptr, const int32_t* inc_ptr,
-                                 const int32_t* inc_elem, const uint32_t* inc_code, int max_degree, int mode,
-                                 int precision, double* f_out, void* k_out, void* status, void* stream) {
+extern "C" int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t chunk_elems, int64_t* ring_elems,
+                              int64_t* bytes) {
   using namespace psx;
-  if (!conn || !X || !nbr_ptr || !inc_ptr || !inc_elem || !inc_code || !status) return PSX_ERR_ARG;
-  if (E <= 0 || N <= 0 || N >= (int64_t)0x7fffffff || E >= (int64_t)0x7fffffff) return PSX_ERR_ARG;
-  if (max_degree > PSX_TET4_MAX_DEGREE) return PSX_ERR_LIMIT;
+  if (!plan_ok(plan) || !ring_elems || !bytes) return PSX_ERR_ARG;
+  if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  if (chunk_elems <= 0 || chunk_elems % plan->granule) return PSX_ERR_ARG;
+  const int64_t ring = ring_elems_for(plan, chunk_elems);
+  const int kt = precision == PSX_FP64 ? 8 : 4;
+  const int kK = plan->npe == 4 ? RecLayout<4>::kK : RecLayout<10>::kK;
+  const int kF = plan->npe == 4 ? RecLayout<4>::kF : RecLayout<10>::kF;
+  *ring_elems = ring;
+  *bytes = ring * (int64_t)(kK * kt + kF * 8) + 256;
+  return PSX_OK;
+}
+
+extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
+                                 const double* kappa_e, double mu, double kappa, double lam, int mode,
+                                 int precision, int64_t chunk_elems, double* f_out, void* k_out, void* work,
+                                 int64_t work_bytes, void* status, void* stream) {
+  using namespace psx;
+  if (!plan_ok(plan) || plan->npe != 4 || !X || !status || !work) return PSX_ERR_ARG;
   if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
   const bool wantF = (mode & PSX_WANT_F) != 0, wantK = (mode & PSX_WANT_K) != 0,
              linear = (mode & PSX_LINEAR) != 0;
   if (linear && (wantF || wantK || !k_out)) return PSX_ERR_ARG;
   if (!linear && (!(wantF || wantK) || !u)) return PSX_ERR_ARG;
   if (wantF && !f_out) return PSX_ERR_ARG;
-  if ((wantK || linear) && !k_out) return PSX_ERR_ARG;
+  if (wantK && !k_out) return PSX_ERR_ARG;
+  int64_t ring = 0, need = 0;
+  int rc = psx_work_bytes(plan, precision, chunk_elems, &ring, &need);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < need || (reinterpret_cast<uintptr_t>(work) & 255)) return PSX_ERR_ARG;
+  const int kt = precision == PSX_FP64 ? 8 : 4;
+  char* w = static_cast<char*>(work);
+  void* krec = w;
+  double* frec = reinterpret_cast<double*>(w + ((ring * RecLayout<4>::kK * kt + 255) / 256) * 256);
+  if ((char*)(frec + ring * RecLayout<4>::kF) > w + work_bytes) return PSX_ERR_ARG;
+  Tet4Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define PSX_T4(KT, M) \
-  launch_tet4<KT, M>(conn, X, u, mu_e, kappa_e, mu, kappa, lam, N, nbr_ptr, inc_ptr, inc_elem, inc_code, f_out, k_out, status, s)
+  run_tet4<KT, M>(plan, A, chunk_elems, ring, static_cast<KT*>(krec), frec, static_cast<KT*>(k_out), f_out, s)
   if (linear) return precision == PSX_FP64 ? PSX_T4(double, PSX_LINEAR) : PSX_T4(float, PSX_LINEAR);
   if (wantF && wantK)
     return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_F | PSX_WANT_K) : PSX_T4(float, PSX_WANT_F | PSX_WANT_K);

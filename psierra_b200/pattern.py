@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from psierra_b200 import _lib
 from psierra_b200._lib import check, lib, ptr
 
 
@@ -43,6 +44,7 @@ class MeshPattern:
         self.max_degree = int(deg.max()) if N else 0
         self._dev: dict | None = None
         self._blocks: tuple | None = None
+        self._plan_host: dict | None = None
 
     @property
     def n_dofs(self) -> int:
@@ -60,6 +62,38 @@ class MeshPattern:
             self._blocks = (blk_ptr, blk_src)
         return self._blocks
 
+    GRANULE = 4096
+
+    def plan_host(self) -> dict:
+        """Host arrays of the gather plan (``psx_plan_fill``), built once."""
+        if self._plan_host is None:
+            L = lib()
+            E, npe, N = self.n_elements, self.npe, self.n_nodes
+            n_pairs = np.zeros(1, dtype=np.int64)
+            n_src = np.zeros(1, dtype=np.int64)
+            check(L.psx_plan_count(ptr(self.conn), E, npe, N, ptr(self.nbr_ptr), ptr(n_pairs), ptr(n_src)),
+                  "psx_plan_count")
+            P, S = int(n_pairs[0]), int(n_src[0])
+            ng = (E + self.GRANULE - 1) // self.GRANULE
+            h = {
+                "pair_info": np.zeros(4 * max(P, 1), dtype=np.int32),
+                "pair_ptr": np.zeros(P + 1, dtype=np.int32),
+                "pair_src": np.zeros(max(S, 1), dtype=np.int32),
+                "pair_gptr": np.zeros(ng + 1, dtype=np.int32),
+                "node_info": np.zeros(4 * N, dtype=np.int32),
+                "node_ptr": np.zeros(N + 1, dtype=np.int32),
+                "node_src": np.zeros(E * npe, dtype=np.int32),
+                "node_gptr": np.zeros(ng + 1, dtype=np.int32),
+                "max_span": np.zeros(1, dtype=np.int64),
+            }
+            check(L.psx_plan_fill(ptr(self.conn), E, npe, N, ptr(self.nbr_ptr), ptr(self.nbr), self.GRANULE,
+                                  ptr(h["pair_info"]), ptr(h["pair_ptr"]), ptr(h["pair_src"]), ptr(h["pair_gptr"]),
+                                  ptr(h["node_info"]), ptr(h["node_ptr"]), ptr(h["node_src"]), ptr(h["node_gptr"]),
+                                  ptr(h["max_span"])), "psx_plan_fill")
+            h["n_pairs"], h["n_granules"] = P, ng
+            self._plan_host = h
+        return self._plan_host
+
     def device(self, device) -> dict:
         """Device copies of the arrays the kernels read (uploaded once)."""
         import torch
@@ -76,5 +110,17 @@ class MeshPattern:
                 "indptr": t(self.indptr),
                 "indices": t(self.indices),
             }
+            h = self.plan_host()
+            for k in ("pair_info", "pair_ptr", "pair_src", "node_info", "node_ptr", "node_src"):
+                d[k] = t(h[k])
+            st = _lib.PlanStruct()
+            st.npe, st.n_granules = self.npe, h["n_granules"]
+            st.n_elements, st.n_nodes, st.n_pairs = self.n_elements, self.n_nodes, h["n_pairs"]
+            st.granule, st.max_span = self.GRANULE, int(h["max_span"][0])
+            for k in ("conn", "pair_info", "pair_ptr", "pair_src", "node_info", "node_ptr", "node_src"):
+                setattr(st, k, d[k].data_ptr())
+            st.pair_gptr = h["pair_gptr"].ctypes.data
+            st.node_gptr = h["node_gptr"].ctypes.data
+            d["plan"] = st
             self._dev = d
         return self._dev
