@@ -157,6 +157,12 @@ def time_steps(fn, steps: int, warmup: int, sync_all):
 
     for _ in range(warmup):
         fn()
+    # keep warming until the clocks have ramped (at least 0.5 s of work)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < 0.5:
+        fn()
+        torch.cuda.synchronize()
     sync_all()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)

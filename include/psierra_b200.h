@@ -131,6 +131,14 @@ typedef struct psx_plan {
   const int32_t* node_src;  /* device, e * 16 + local node index */
   const int32_t* pair_gptr; /* host, n_granules + 1: pair items ready in each granule */
   const int32_t* node_gptr; /* host, n_granules + 1 */
+  int32_t tile;             /* items per task (psx_task_fill) */
+  int32_t pad_;
+  int64_t n_tasks_k;        /* task queue with pair tiles (any request involving K) */
+  int64_t n_tasks_f;        /* task queue without pair tiles (f only) */
+  const int32_t* tasks_k;   /* device, 4 per task: kind, granule, begin, end */
+  const int32_t* tasks_f;   /* device */
+  const int32_t* btiles_k;  /* device, n_granules: gather tiles per granule in tasks_k */
+  const int32_t* btiles_f;  /* device, n_granules: gather tiles per granule in tasks_f */
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */
@@ -149,11 +157,21 @@ int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int3
                   int32_t* node_src, int32_t* node_gptr, int64_t* max_span);
 
 /*
- * Workspace the assembly needs for chunks of `chunk_elems` elements (a multiple of
- * the plan granule): a ring of element records, *ring_elems records long.
+ * Task queue of the persistent assembly kernel (host): for each granule g, the
+ * element tiles of g followed by the gather tiles made ready by granule g-1 (pairs
+ * when with_pairs, then nodes).  Each task is 4 int32 {kind, granule, begin, end};
+ * b_tiles_per_granule (n_granules) counts the gather tiles of each granule.  `tile` must
+ * divide the plan granule.  Uses only the host fields of `plan`.
  */
-int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t chunk_elems, int64_t* ring_elems,
-                   int64_t* bytes);
+int psx_task_count(const psx_plan_t* plan, int with_pairs, int32_t tile, int64_t* n_tasks);
+int psx_task_fill(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t* tasks,
+                  int32_t* b_tiles_per_granule);
+
+/*
+ * Workspace bytes of one assembly call on the current device: task counters and a
+ * ring of *ring_elems element records (K part in the precision's type, f in double).
+ */
+int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t* ring_elems, int64_t* bytes);
 
 /* ---- Tet4 element kernels (device) ----------------------------------------- */
 
@@ -167,14 +185,15 @@ int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t chunk_elems, i
  *   k_out (device, nnz values in psx_csr_pattern order: double for PSX_FP64, float
  *          for PSX_FP32_MIXED) when mode has PSX_WANT_K or PSX_LINEAR
  *   work (device, >= psx_work_bytes, 256-byte aligned) scratch ring of element records
- *   status (device, psx_status_bytes(), zeroed by the caller)
+ *   status (device, psx_status_bytes(), zeroed by the caller); flags bit 0 is set if a
+ *          bounded wait of the persistent kernel gave up (the results are then invalid)
+ * One launch of a persistent kernel; the call also clears the task counters.
  * Deterministic: every output value is a fixed-order sum; no atomics touch f or K.
  */
 int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u,
                       const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,
-                      int mode, int precision, int64_t chunk_elems,
-                      double* f_out, void* k_out, void* work, int64_t work_bytes,
-                      void* status, void* stream);
+                      int mode, int precision, double* f_out, void* k_out, void* work,
+                      int64_t work_bytes, void* status, void* stream);
 
 /*
  * Reference det (of [1 X], = 6 V) and det F of one element, written to out2

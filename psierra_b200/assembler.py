@@ -55,7 +55,6 @@ class GPUAssembler:
         self.status = torch.zeros((nbytes + 3) // 4, dtype=torch.int32, device=self.device)
         self._dets = torch.zeros(2, dtype=torch.float64, device=self.device)
         self._work: dict = {}
-        self.chunk_elems = self.default_chunk(precision)
         self.set_material(material)
 
     # ------------------------------------------------------------------ material
@@ -91,28 +90,19 @@ class GPUAssembler:
         return torch.empty(self.nnz, dtype=self.k_dtype(precision), device=self.device)
 
     # ------------------------------------------------------------------ workspace
-    def default_chunk(self, precision: str) -> int:
-        """Elements per launch: keeps the ring of element records well inside L2."""
-        g = self.pattern.GRANULE
-        c = 32768 if precision == "fp32-mixed" else 16384
-        return max(g, (min(c, self.n_elements + g - 1) // g) * g)
-
     def launches_per_call(self, precision: str | None = None) -> int:
-        """Kernel launches one assemble() call makes (one per element chunk, plus one)."""
-        prec = precision or self.precision
-        chunk = self.chunk_elems if prec == self.precision else self.default_chunk(prec)
-        return (self.n_elements + chunk - 1) // chunk + 1
+        """Kernel launches one assemble() call makes (one persistent kernel)."""
+        return 1
 
-    def workspace(self, precision: str, chunk: int) -> torch.Tensor:
-        key = (precision, chunk)
-        w = self._work.get(key)
+    def workspace(self, precision: str) -> torch.Tensor:
+        w = self._work.get(precision)
         if w is None:
             ring = ctypes.c_int64()
             nbytes = ctypes.c_int64()
-            check(lib().psx_work_bytes(ctypes.byref(self.dev["plan"]), PRECISIONS[precision], chunk,
+            check(lib().psx_work_bytes(ctypes.byref(self.dev["plan"]), PRECISIONS[precision],
                                        ctypes.byref(ring), ctypes.byref(nbytes)), "psx_work_bytes")
             w = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
-            self._work = {key: w}  # keep one workspace alive
+            self._work[precision] = w
         return w
 
     # ------------------------------------------------------------------ kernels
@@ -147,11 +137,10 @@ class GPUAssembler:
         if want_k and k_out.dtype != self.k_dtype(prec):
             raise ValueError(f"k_out must be {self.k_dtype(prec)} for precision {prec}")
         self.status.zero_()
-        chunk = self.chunk_elems if prec == self.precision else self.default_chunk(prec)
-        work = self.workspace(prec, chunk)
+        work = self.workspace(prec)
         rc = lib().psx_tet4_assemble(
             ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u) if not linear else None,
-            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam, mode, PRECISIONS[prec], chunk,
+            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam, mode, PRECISIONS[prec],
             ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(work), work.numel(),
             ptr(self.status), _stream_handle())
         check(rc, "psx_tet4_assemble")
@@ -167,14 +156,16 @@ class GPUAssembler:
         return u.contiguous()
 
     # ------------------------------------------------------------------ status
-    def status_counts(self) -> tuple[int, int, int]:
-        """(n_inverted, n_bad_volume, first_bad_element or -1) of the last sweep (synchronises)."""
-        s = self.status[:3].cpu().numpy()
+    def status_counts(self) -> tuple[int, int, int, int]:
+        """(n_inverted, n_bad_volume, first_bad_element or -1, flags) of the last sweep (synchronises)."""
+        s = self.status[:6].cpu().numpy()
         first = int(0x7FFFFFFF - int(s[2])) if s[2] != 0 else -1
-        return int(s[0]), int(s[1]), first
+        return int(s[0]), int(s[1]), first, int(s[5])
 
     def raise_on_bad_elements(self, u: torch.Tensor | None) -> None:
-        n_inv, n_vol, first = self.status_counts()
+        n_inv, n_vol, first, flags = self.status_counts()
+        if flags & 1:
+            raise RuntimeError("psierra_b200: a bounded wait in the assembly kernel gave up; results are invalid")
         if n_inv == 0 and n_vol == 0:
             return
         check(lib().psx_tet4_element_dets(ptr(self.dev["conn"]), ptr(self.X), ptr(u), first,

@@ -1,10 +1,10 @@
 // Owner-computes gather of element records into the CSR values and f (kernel "B").
 //
-// The element kernel writes, per element e, a record into a ring of scratch slots
+// The element phase writes, per element e, a record into a ring of scratch slots
 // (slot = e & ring_mask):
-//   K part (KT): npair off-diagonal 3x3 blocks, 12 values each (9 used), oriented with
-//                rows = the element node of smaller global id; then npe diagonal blocks,
-//                8 values each (xx xy xz yy yz zz + 2 pad).  npair = npe (npe - 1) / 2.
+//   K part (KT): npair off-diagonal 3x3 blocks, 9 values each, oriented with rows = the
+//                element node of smaller global id; then npe diagonal blocks, 6 values
+//                each (xx xy xz yy yz zz).  npair = npe (npe - 1) / 2.
 //   f part (double): 3 values per element node.
 // A pair item (i < j) sums the blocks of every element holding both nodes, in
 // ascending element order, and writes K_ij (row 3i+k, upper) and its transpose K_ji
@@ -21,10 +21,10 @@ namespace psx {
 template <int NPE>
 struct RecLayout {
   static constexpr int kPairs = NPE * (NPE - 1) / 2;
-  static constexpr int kK = kPairs * 12 + NPE * 8;  // KT values per element record
-  static constexpr int kF = NPE * 3;                 // doubles per element f record
-  __host__ __device__ static constexpr int pair_off(int slot) { return slot * 12; }
-  __host__ __device__ static constexpr int diag_off(int a) { return kPairs * 12 + a * 8; }
+  static constexpr int kK = kPairs * 9 + NPE * 6;  // KT values per element record
+  static constexpr int kF = NPE * 3;                // doubles per element f record
+  __host__ __device__ static constexpr int pair_off(int slot) { return slot * 9; }
+  __host__ __device__ static constexpr int diag_off(int a) { return kPairs * 9 + a * 6; }
 };
 
 struct GatherArgs {
@@ -39,42 +39,10 @@ struct GatherArgs {
   int64_t ring_mask;
 };
 
-template <typename KT>
-__device__ __forceinline__ void load12(const KT* __restrict__ p, KT v[12]) {
-  if constexpr (sizeof(KT) == 4) {
-    const float4* q = reinterpret_cast<const float4*>(p);
+template <typename KT, int N>
+__device__ __forceinline__ void load_cg(const KT* __restrict__ p, KT v[N]) {
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      float4 t = __ldcg(q + i);
-      v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
-    }
-  } else {
-    const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      double2 t = __ldcg(q + i);
-      v[2 * i] = t.x; v[2 * i + 1] = t.y;
-    }
-  }
-}
-
-template <typename KT>
-__device__ __forceinline__ void load8(const KT* __restrict__ p, KT v[8]) {
-  if constexpr (sizeof(KT) == 4) {
-    const float4* q = reinterpret_cast<const float4*>(p);
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      float4 t = __ldcg(q + i);
-      v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
-    }
-  } else {
-    const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      double2 t = __ldcg(q + i);
-      v[2 * i] = t.x; v[2 * i + 1] = t.y;
-    }
-  }
+  for (int i = 0; i < N; ++i) v[i] = __ldcg(p + i);
 }
 
 // Pair item: off-diagonal block and its transpose.
@@ -91,8 +59,8 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
     const int32_t src = __ldg(g.pair_src + s);
     const int64_t e = src >> 6;
     const int slot = src & 63;
-    KT v[12];
-    load12<KT>(krec + (e & g.ring_mask) * L::kK + L::pair_off(slot), v);
+    KT v[9];
+    load_cg<KT, 9>(krec + (e & g.ring_mask) * L::kK + L::pair_off(slot), v);
 #pragma unroll
     for (int j = 0; j < 9; ++j) acc[j] += v[j];
   }
@@ -123,8 +91,8 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
     const int a = src & 15;
     const int64_t slot = e & g.ring_mask;
     if constexpr (WANT_K) {
-      KT v[8];
-      load8<KT>(krec + slot * L::kK + L::diag_off(a), v);
+      KT v[6];
+      load_cg<KT, 6>(krec + slot * L::kK + L::diag_off(a), v);
 #pragma unroll
       for (int j = 0; j < 6; ++j) acc[j] += v[j];
     }
@@ -151,40 +119,139 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
   }
 }
 
-// Store a 12-value off-diagonal block record (9 used), transposed when `swap`.
+// Store an off-diagonal block record (9 values), transposed when `swap`.
 template <typename KT>
 __device__ __forceinline__ void store_pair_block(KT* __restrict__ dst, const KT b[9], bool swap) {
-  KT o[12];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
-    for (int m = 0; m < 3; ++m) o[3 * k + m] = swap ? b[3 * m + k] : b[3 * k + m];
-  o[9] = o[10] = o[11] = (KT)0;
-  if constexpr (sizeof(KT) == 4) {
-    float4* q = reinterpret_cast<float4*>(dst);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) __stcg(q + i, make_float4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]));
-  } else {
-    double2* q = reinterpret_cast<double2*>(dst);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) __stcg(q + i, make_double2(o[2 * i], o[2 * i + 1]));
-  }
+    for (int m = 0; m < 3; ++m) __stcg(dst + 3 * k + m, swap ? b[3 * m + k] : b[3 * k + m]);
 }
 
-// Store a diagonal block record: xx xy xz yy yz zz (+2 pad).
+// Store a diagonal block record: xx xy xz yy yz zz.
 template <typename KT>
 __device__ __forceinline__ void store_diag_block(KT* __restrict__ dst, const KT d[6]) {
-  if constexpr (sizeof(KT) == 4) {
-    float4* q = reinterpret_cast<float4*>(dst);
-    __stcg(q, make_float4(d[0], d[1], d[2], d[3]));
-    __stcg(q + 1, make_float4(d[4], d[5], 0.f, 0.f));
-  } else {
-    double2* q = reinterpret_cast<double2*>(dst);
-    __stcg(q, make_double2(d[0], d[1]));
-    __stcg(q + 1, make_double2(d[2], d[3]));
-    __stcg(q + 2, make_double2(d[4], d[5]));
-    __stcg(q + 3, make_double2(0.0, 0.0));
+#pragma unroll
+  for (int i = 0; i < 6; ++i) __stcg(dst + i, d[i]);
+}
+
+// ---- persistent task queue --------------------------------------------------------
+// Counters live at the start of the workspace: [0] next task, [1 .. G] element tiles
+// finished per granule, [1 + G .. 2G] gather tiles finished per granule.
+struct QueueArgs {
+  const int4* tasks;
+  int32_t n_tasks;
+  int32_t n_granules;
+  const int32_t* btiles;  // gather tiles per granule
+  int32_t* counters;
+  int32_t granule_log2;
+  int32_t tile;
+  int32_t span_g;         // max item span in granules (rounded up)
+  int32_t ring_g;         // ring length in granules (power of two)
+  int64_t n_elements;
+};
+
+__device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded wait, executed by warp 0 of the block: lane j checks counter[first + j] >=
+// target(first + j) for j < count.  Returns false (and flags the status) if the wait
+// gives up; the caller then still proceeds, so every access stays in bounds and the
+// host reports the failure.
+template <typename Target>
+__device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first, int32_t count, Target target,
+                                              Status* st) {
+  const int lane = threadIdx.x & 31;
+  constexpr int kMaxSpins = 1 << 22;
+  for (int32_t base = 0; base < count; base += 32) {
+    const int32_t g = first + base + lane;
+    const bool mine = (base + lane) < count && g >= 0;
+    const int32_t want = mine ? target(g) : 0;
+    int spins = 0;
+    while (true) {
+      const bool ok = !mine || ld_acquire(cnt + g) >= want;
+      if (__all_sync(0xffffffffu, ok)) break;
+      // once any wait has given up, every later wait returns at once
+      if (++spins > kMaxSpins || (ld_acquire(&st->flags) & 1)) {
+        if (lane == 0) atomicOr(&st->flags, 1);
+        return false;
+      }
+      if (spins > 64) __nanosleep(200);
+    }
   }
+  return true;
+}
+
+
+// ---- workspace layout (host side) ---------------------------------------------------
+struct WorkLayout {
+  int32_t* counters;
+  size_t counter_bytes;
+  void* krec;
+  double* frec;
+  int64_t ring_elems;
+  int32_t ring_g;
+  int32_t span_g;
+  int32_t granule_log2;
+  int32_t grid;
+  int64_t total_bytes;
+};
+
+inline int32_t device_sm_count() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  return sms;
+}
+
+// Workspace of one assembly call: task counters, then the ring of K records, then the
+// ring of f records (each 256-byte aligned).  The ring spans a power-of-two number of
+// granules covering the item span plus the blocks in flight; with `work` null only the
+// sizes are computed.
+inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayout* W) {
+  if (!P || !W || P->n_elements <= 0 || P->n_nodes <= 0 || P->granule <= 0 || (P->granule & (P->granule - 1)))
+    return PSX_ERR_ARG;
+  if (!P->conn || !P->pair_info || !P->pair_ptr || !P->pair_src || !P->node_info || !P->node_ptr ||
+      !P->node_src || !P->tasks_k || !P->tasks_f || !P->btiles_k || !P->btiles_f || P->tile <= 0)
+    return PSX_ERR_ARG;
+  if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  if (P->npe != 4 && P->npe != 10) return PSX_ERR_ARG;
+  const int kt = precision == PSX_FP64 ? 8 : 4;
+  const int kK = P->npe == 4 ? RecLayout<4>::kK : RecLayout<10>::kK;
+  const int kF = P->npe == 4 ? RecLayout<4>::kF : RecLayout<10>::kF;
+  int32_t lg = 0;
+  while (((int64_t)1 << lg) < P->granule) ++lg;
+  W->granule_log2 = lg;
+  W->span_g = (int32_t)((P->max_span + P->granule - 1) / P->granule);
+  int32_t all = 1;
+  while (all < P->n_granules) all <<= 1;
+  int32_t ring = 1;
+  while (ring < W->span_g + 12) ring <<= 1;
+  W->ring_g = ring < all ? ring : all;
+  W->ring_elems = (int64_t)W->ring_g * P->granule;
+  const int sms = device_sm_count();
+  if (sms <= 0) return PSX_ERR_CUDA;
+  const int64_t ntask = P->n_tasks_k > P->n_tasks_f ? P->n_tasks_k : P->n_tasks_f;
+  W->grid = (int32_t)(sms * 4 < ntask ? sms * 4 : ntask);
+  auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
+  W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
+  const int64_t kbytes = up(W->ring_elems * kK * kt);
+  const int64_t fbytes = up(W->ring_elems * kF * 8);
+  W->total_bytes = (int64_t)W->counter_bytes + kbytes + fbytes;
+  W->counters = nullptr;
+  W->krec = nullptr;
+  W->frec = nullptr;
+  if (work) {
+    if (reinterpret_cast<uintptr_t>(work) & 255) return PSX_ERR_ARG;
+    char* w = static_cast<char*>(work);
+    W->counters = reinterpret_cast<int32_t*>(w);
+    W->krec = w + W->counter_bytes;
+    W->frec = reinterpret_cast<double*>(w + W->counter_bytes + kbytes);
+  }
+  return PSX_OK;
 }
 
 }  // namespace psx

@@ -313,3 +313,62 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
   }
   return PSX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Task queue of the persistent assembly kernel: for each granule g, the element
+// tiles of g followed by the gather tiles made ready by granule g-1 (pairs, then
+// nodes); the gather tiles of the last granule close the queue.  Task = int4
+// {kind, granule, begin, end}: kind 0 = element tile [begin, end), 1 = pair items,
+// 2 = node items.  `with_pairs` = 0 builds the f-only queue (no pair tiles).
+extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile, int64_t* n_tasks) {
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || !n_tasks) return PSX_ERR_ARG;
+  int64_t n = 0;
+  const int64_t G = P->n_granules;
+  for (int64_t g = 0; g <= G; ++g) {
+    if (g < G) {
+      const int64_t e0 = g * P->granule, e1 = std::min<int64_t>(P->n_elements, e0 + P->granule);
+      n += (e1 - e0 + tile - 1) / tile;
+    }
+    if (g >= 1) {
+      const int64_t r = g - 1;
+      if (with_pairs) n += (P->pair_gptr[r + 1] - P->pair_gptr[r] + tile - 1) / tile;
+      const int64_t n0 = r == 0 ? 0 : P->node_gptr[r];
+      n += (P->node_gptr[r + 1] - n0 + tile - 1) / tile;
+    }
+  }
+  *n_tasks = n;
+  return PSX_OK;
+}
+
+extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t* tasks,
+                             int32_t* b_tiles_per_granule) {
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || !tasks || !b_tiles_per_granule)
+    return PSX_ERR_ARG;
+  const int64_t G = P->n_granules;
+  int64_t k = 0;
+  auto push = [&](int32_t kind, int64_t g, int64_t b, int64_t e) {
+    tasks[4 * k + 0] = kind;
+    tasks[4 * k + 1] = (int32_t)g;
+    tasks[4 * k + 2] = (int32_t)b;
+    tasks[4 * k + 3] = (int32_t)e;
+    ++k;
+  };
+  for (int64_t g = 0; g <= G; ++g) {
+    if (g < G) {
+      const int64_t e0 = g * P->granule, e1 = std::min<int64_t>(P->n_elements, e0 + P->granule);
+      for (int64_t b = e0; b < e1; b += tile) push(0, g, b, std::min<int64_t>(e1, b + tile));
+    }
+    if (g >= 1) {
+      const int64_t r = g - 1;
+      int32_t nb = 0;
+      if (with_pairs)
+        for (int64_t b = P->pair_gptr[r]; b < P->pair_gptr[r + 1]; b += tile, ++nb)
+          push(1, r, b, std::min<int64_t>(P->pair_gptr[r + 1], b + tile));
+      const int64_t n0 = r == 0 ? 0 : P->node_gptr[r];
+      for (int64_t b = n0; b < P->node_gptr[r + 1]; b += tile, ++nb)
+        push(2, r, b, std::min<int64_t>(P->node_gptr[r + 1], b + tile));
+      b_tiles_per_granule[r] = nb;
+    }
+  }
+  return PSX_OK;
+}

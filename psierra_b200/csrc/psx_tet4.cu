@@ -13,8 +13,8 @@
 //   B (owner-computes gather): one thread per node pair / node sums the records of the
 //     elements that share it, in ascending element order, and writes each CSR value and
 //     each f entry exactly once.
-// Launch k runs A on element chunk k and B on the items completed by chunk k-1, so the
-// two overlap and the ring only ever holds a few chunks.  No atomics touch f or K, so
+// Both phases run in one persistent launch that drains a task queue in mesh order, so
+// the ring only holds the elements still awaited by some gather item.  No atomics touch f or K, so
 // results are bitwise reproducible run to run.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -195,32 +195,71 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   }
 }
 
+// Persistent assembly kernel: each block repeatedly claims the next task of the queue
+// (psx_task_fill).  Element tiles publish their granule's completion count; gather
+// tiles wait for the element granules they read; element tiles wait until the gather
+// tiles still reading the ring slots they overwrite are done.  Every wait is on tasks
+// that earlier blocks have already claimed, so the queue always drains.
 template <typename KT, int MODE>
 __global__ void __launch_bounds__(kThreads, 4)
-tet4_fused_kernel(Tet4Args A, GatherArgs g, int64_t e0, int64_t e1, int32_t nA, int32_t nP,
-                  KT* __restrict__ krec, double* __restrict__ frec, KT* __restrict__ k_out,
-                  double* __restrict__ f_out) {
+tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
+                       KT* __restrict__ k_out, double* __restrict__ f_out) {
   using L = RecLayout<4>;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
-  int32_t b = blockIdx.x;
-  if (b < nA) {
-    const int64_t e = e0 + (int64_t)b * kThreads + threadIdx.x;
-    if (e < e1) {
-      const int64_t slot = e & g.ring_mask;
-      tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
+  __shared__ int4 s_task;
+  int32_t* acnt = Q.counters + 1;
+  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
+  const int64_t gsize = (int64_t)1 << Q.granule_log2;
+  auto atiles = [&](int32_t r) -> int32_t {
+    const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
+    return (int32_t)((n + Q.tile - 1) / Q.tile);
+  };
+  auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  while (true) {
+    if (threadIdx.x == 0) {
+      const int32_t t = atomicAdd(Q.counters, 1);
+      s_task = t < Q.n_tasks ? __ldg(Q.tasks + t) : make_int4(-1, 0, 0, 0);
     }
-    return;
+    __syncthreads();
+    const int4 task = s_task;
+    __syncthreads();
+    if (task.x < 0) break;
+    const int32_t gr = task.y;
+    if (task.x == 0) {
+      const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
+      if (old >= 0 && threadIdx.x < 32) {
+        const int32_t cnt = min(Q.span_g + 2, Q.n_granules - old);
+        wait_counters(bcnt, old, cnt, btiles, A.st);
+      }
+      __syncthreads();
+      const int64_t e = task.z + (int64_t)threadIdx.x;
+      if (e < task.w) {
+        const int64_t slot = e & g.ring_mask;
+        tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicAdd(acnt + gr, 1);
+    } else {
+      if (threadIdx.x < 32) {
+        const int32_t first = max(0, gr - Q.span_g - 1);
+        wait_counters(acnt, first, gr - first + 1, atiles, A.st);
+      }
+      __syncthreads();
+      const int32_t item = task.z + threadIdx.x;
+      if (item < task.w) {
+        if (task.x == 1) {
+          gather_pair<KT, 4>(g, item, krec, k_out);
+        } else {
+          gather_node<KT, 4, kWantK, kWantF>(g, item, krec, frec, k_out, f_out);
+        }
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicAdd(bcnt + gr, 1);
+    }
   }
-  b -= nA;
-  if (b < nP) {
-    const int32_t p = g.p0 + b * kThreads + threadIdx.x;
-    if (p < g.p1) gather_pair<KT, 4>(g, p, krec, k_out);
-    return;
-  }
-  b -= nP;
-  const int32_t n = g.n0 + b * kThreads + threadIdx.x;
-  if (n < g.n1) gather_node<KT, 4, kWantK, kWantF>(g, n, krec, frec, k_out, f_out);
 }
 
 __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
@@ -245,12 +284,9 @@ __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double*
 }
 
 template <typename KT, int MODE>
-int run_tet4(const psx_plan_t* P, const Tet4Args& A, int64_t chunk, int64_t ring, KT* krec, double* frec,
-             KT* k_out, double* f_out, cudaStream_t stream) {
+int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
+             cudaStream_t stream) {
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
-  const int64_t E = P->n_elements;
-  const int64_t G = chunk / P->granule;  // granules per chunk
-  const int64_t n_chunks = (E + chunk - 1) / chunk;
   GatherArgs g;
   g.pair_info = P->pair_info;
   g.pair_ptr = P->pair_ptr;
@@ -258,105 +294,60 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, int64_t chunk, int64_t ring
   g.node_info = P->node_info;
   g.node_ptr = P->node_ptr;
   g.node_src = P->node_src;
-  g.ring_mask = ring - 1;
-  for (int64_t k = 0; k <= n_chunks; ++k) {
-    int64_t e0 = 0, e1 = 0;
-    int32_t nA = 0, nP = 0, nN = 0;
-    if (k < n_chunks) {
-      e0 = k * chunk;
-      e1 = std::min<int64_t>(E, e0 + chunk);
-      nA = (int32_t)((e1 - e0 + kThreads - 1) / kThreads);
-    }
-    g.p0 = g.p1 = g.n0 = g.n1 = 0;
-    if (k >= 1) {
-      const int64_t ga = (k - 1) * G, gb = std::min<int64_t>(k * G, P->n_granules);
-      if (kWantK) {
-        g.p0 = P->pair_gptr[ga];
-        g.p1 = P->pair_gptr[gb];
-        nP = (g.p1 - g.p0 + kThreads - 1) / kThreads;
-      }
-      g.n0 = (k == 1) ? 0 : P->node_gptr[ga];
-      g.n1 = P->node_gptr[gb];
-      nN = (g.n1 - g.n0 + kThreads - 1) / kThreads;
-    }
-    const int32_t blocks = nA + nP + nN;
-    if (blocks == 0) continue;
-    tet4_fused_kernel<KT, MODE><<<blocks, kThreads, 0, stream>>>(A, g, e0, e1, nA, nP, krec, frec, k_out, f_out);
-    PSX_CUDA_CHECK_LAUNCH();
-  }
+  g.p0 = g.p1 = g.n0 = g.n1 = 0;
+  g.ring_mask = W.ring_elems - 1;
+  QueueArgs Q;
+  Q.tasks = reinterpret_cast<const int4*>(kWantK ? P->tasks_k : P->tasks_f);
+  Q.n_tasks = (int32_t)(kWantK ? P->n_tasks_k : P->n_tasks_f);
+  Q.n_granules = P->n_granules;
+  Q.btiles = kWantK ? P->btiles_k : P->btiles_f;
+  Q.counters = W.counters;
+  Q.granule_log2 = W.granule_log2;
+  Q.tile = P->tile;
+  Q.span_g = W.span_g;
+  Q.ring_g = W.ring_g;
+  Q.n_elements = P->n_elements;
+  if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
+  tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, 0, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
+                                                                   k_out, f_out);
+  PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }
 
 }  // namespace
 }  // namespace psx
 
-namespace {
-
-// Ring of element records: a power of two covering the chunk being written, the
-// chunk being gathered and the item span behind it.
-int64_t ring_elems_for(const psx_plan_t* P, int64_t chunk) {
-  const int64_t need = (P->max_span + chunk - 1) / chunk + 2;
-  int64_t ring = 1;
-  while (ring < need * chunk) ring <<= 1;
-  const int64_t full = [&] {
-    int64_t r = 1;
-    while (r < P->n_elements) r <<= 1;
-    return r;
-  }();
-  return std::min(ring, full);
-}
-
-bool plan_ok(const psx_plan_t* P) {
-  return P && P->conn && P->pair_info && P->pair_ptr && P->pair_src && P->node_info && P->node_ptr &&
-         P->node_src && P->pair_gptr && P->node_gptr && P->n_elements > 0 && P->n_nodes > 0 && P->granule > 0 &&
-         (P->granule & (P->granule - 1)) == 0;
-}
-
-}  // namespace
-
 extern "C" size_t psx_status_bytes(void) { return sizeof(psx::Status); }
 
-extern "C" int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t chunk_elems, int64_t* ring_elems,
-                              int64_t* bytes) {
-  using namespace psx;
-  if (!plan_ok(plan) || !ring_elems || !bytes) return PSX_ERR_ARG;
-  if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
-  if (chunk_elems <= 0 || chunk_elems % plan->granule) return PSX_ERR_ARG;
-  const int64_t ring = ring_elems_for(plan, chunk_elems);
-  const int kt = precision == PSX_FP64 ? 8 : 4;
-  const int kK = plan->npe == 4 ? RecLayout<4>::kK : RecLayout<10>::kK;
-  const int kF = plan->npe == 4 ? RecLayout<4>::kF : RecLayout<10>::kF;
-  *ring_elems = ring;
-  *bytes = ring * (int64_t)(kK * kt + kF * 8) + 256;
+extern "C" int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t* ring_elems, int64_t* bytes) {
+  psx::WorkLayout W;
+  const int rc = psx::work_layout(plan, precision, nullptr, &W);
+  if (rc != PSX_OK) return rc;
+  if (!ring_elems || !bytes) return PSX_ERR_ARG;
+  *ring_elems = W.ring_elems;
+  *bytes = W.total_bytes;
   return PSX_OK;
 }
 
 extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
                                  const double* kappa_e, double mu, double kappa, double lam, int mode,
-                                 int precision, int64_t chunk_elems, double* f_out, void* k_out, void* work,
-                                 int64_t work_bytes, void* status, void* stream) {
+                                 int precision, double* f_out, void* k_out, void* work, int64_t work_bytes,
+                                 void* status, void* stream) {
   using namespace psx;
-  if (!plan_ok(plan) || plan->npe != 4 || !X || !status || !work) return PSX_ERR_ARG;
-  if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  if (!plan || plan->npe != 4 || !X || !status || !work) return PSX_ERR_ARG;
   const bool wantF = (mode & PSX_WANT_F) != 0, wantK = (mode & PSX_WANT_K) != 0,
              linear = (mode & PSX_LINEAR) != 0;
   if (linear && (wantF || wantK || !k_out)) return PSX_ERR_ARG;
   if (!linear && (!(wantF || wantK) || !u)) return PSX_ERR_ARG;
   if (wantF && !f_out) return PSX_ERR_ARG;
   if (wantK && !k_out) return PSX_ERR_ARG;
-  int64_t ring = 0, need = 0;
-  int rc = psx_work_bytes(plan, precision, chunk_elems, &ring, &need);
+  WorkLayout W;
+  int rc = work_layout(plan, precision, work, &W);
   if (rc != PSX_OK) return rc;
-  if (work_bytes < need || (reinterpret_cast<uintptr_t>(work) & 255)) return PSX_ERR_ARG;
-  const int kt = precision == PSX_FP64 ? 8 : 4;
-  char* w = static_cast<char*>(work);
-  void* krec = w;
-  double* frec = reinterpret_cast<double*>(w + ((ring * RecLayout<4>::kK * kt + 255) / 256) * 256);
-  if ((char*)(frec + ring * RecLayout<4>::kF) > w + work_bytes) return PSX_ERR_ARG;
+  if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-#define PSX_T4(KT, M) \
-  run_tet4<KT, M>(plan, A, chunk_elems, ring, static_cast<KT*>(krec), frec, static_cast<KT*>(k_out), f_out, s)
+#define PSX_T4(KT, M) run_tet4<KT, M>(plan, A, W, static_cast<KT*>(k_out), f_out, s)
   if (linear) return precision == PSX_FP64 ? PSX_T4(double, PSX_LINEAR) : PSX_T4(float, PSX_LINEAR);
   if (wantF && wantK)
     return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_F | PSX_WANT_K) : PSX_T4(float, PSX_WANT_F | PSX_WANT_K);

@@ -8,6 +8,8 @@ values array in this order is the reference's ``K_tan.data``.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from psierra_b200 import _lib
@@ -63,6 +65,7 @@ class MeshPattern:
         return self._blocks
 
     GRANULE = 4096
+    TILE = 128
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
@@ -121,6 +124,19 @@ class MeshPattern:
                 setattr(st, k, d[k].data_ptr())
             st.pair_gptr = h["pair_gptr"].ctypes.data
             st.node_gptr = h["node_gptr"].ctypes.data
+            st.tile = self.TILE
+            L = lib()
+            for key, with_pairs in (("k", 1), ("f", 0)):
+                nt = ctypes.c_int64()
+                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.TILE, ctypes.byref(nt)), "psx_task_count")
+                tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
+                btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
+                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.TILE, ptr(tasks), ptr(btiles)),
+                      "psx_task_fill")
+                d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
+                setattr(st, "n_tasks_" + key, int(nt.value))
+                setattr(st, "tasks_" + key, d["tasks_" + key].data_ptr())
+                setattr(st, "btiles_" + key, d["btiles_" + key].data_ptr())
             d["plan"] = st
             self._dev = d
         return self._dev

@@ -1,0 +1,87 @@
+"""Deadlock freedom and ring safety of the persistent assembly kernel's task queue (CPU).
+
+The kernel's wait rules, restated:
+* an element tile of granule g waits for all gather tiles of granules
+  [g - R, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
+  slots of granule g - R, if g - R >= 0;
+* a gather tile of granule r waits for all element tiles of granules [r - span_g - 1, r].
+Tasks are claimed in queue order by running blocks, so the queue always drains if every
+task only waits on tasks strictly earlier in the queue.  Ring safety: every gather item
+that reads an element of granule q belongs to a granule in [q, q + span_g + 1].
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from psierra_b200 import _lib, meshgen
+from psierra_b200.pattern import MeshPattern
+
+
+def _queue(p: MeshPattern, with_pairs: int, tile: int):
+    h = p.plan_host()
+    st = _lib.PlanStruct()
+    st.npe, st.n_granules = p.npe, h["n_granules"]
+    st.n_elements, st.n_nodes, st.n_pairs = p.n_elements, p.n_nodes, h["n_pairs"]
+    st.granule, st.max_span = p.GRANULE, int(h["max_span"][0])
+    st.pair_gptr, st.node_gptr = h["pair_gptr"].ctypes.data, h["node_gptr"].ctypes.data
+    L = _lib.lib()
+    nt = ctypes.c_int64()
+    _lib.check(L.psx_task_count(ctypes.byref(st), with_pairs, tile, ctypes.byref(nt)), "count")
+    tasks = np.zeros(4 * nt.value, dtype=np.int32)
+    bt = np.zeros(h["n_granules"], dtype=np.int32)
+    _lib.check(L.psx_task_fill(ctypes.byref(st), with_pairs, tile, _lib.ptr(tasks), _lib.ptr(bt)), "fill")
+    return tasks.reshape(-1, 4), bt, h
+
+
+@pytest.mark.parametrize("granule,with_pairs", [(256, 1), (256, 0), (512, 1), (128, 1)])
+def test_waits_only_on_earlier_tasks(granule, with_pairs):
+    m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
+    p = MeshPattern(m.elements, m.n_nodes)
+    p.GRANULE = granule
+    tile = 64
+    tasks, bt, h = _queue(p, with_pairs, tile)
+    G = h["n_granules"]
+    span_g = -(-int(h["max_span"][0]) // granule)
+    # all items covered exactly once
+    kinds = tasks[:, 0]
+    assert tasks[kinds == 0, 3].sum() - tasks[kinds == 0, 2].sum() == m.n_elements
+    assert tasks[kinds == 2, 3].sum() - tasks[kinds == 2, 2].sum() == m.n_nodes
+    if with_pairs:
+        assert tasks[kinds == 1, 3].sum() - tasks[kinds == 1, 2].sum() == h["n_pairs"]
+    # gather tile counts per granule match
+    for r in range(G):
+        assert bt[r] == np.count_nonzero((kinds != 0) & (tasks[:, 1] == r))
+    # the kernel's ring length (power of two >= span_g + 12, capped to cover all granules)
+    all_g = 1 << int(np.ceil(np.log2(max(G, 1))))
+    ring = 1 << int(np.ceil(np.log2(span_g + 12)))
+    ring = min(ring, all_g)
+    last_a = {}
+    last_b = {}
+    for q, (kind, g, b, e) in enumerate(tasks):
+        if kind == 0:
+            last_a[g] = q
+        else:
+            last_b[g] = q
+    first_pos = {}
+    for q, (kind, g, b, e) in enumerate(tasks):
+        first_pos.setdefault((kind == 0, g), q)
+    for q, (kind, g, b, e) in enumerate(tasks):
+        if kind == 0:
+            old = g - ring
+            if old >= 0:
+                for r in range(old, min(old + span_g + 2, G)):
+                    assert last_b.get(r, -1) < q, "element tile waits on a later gather tile"
+        else:
+            for gp in range(max(0, g - span_g - 1), g + 1):
+                assert last_a[gp] < q, "gather tile waits on a later element tile"
+    # ring safety: items read elements within span_g + 1 granules of their own granule
+    for kind, g, b, e in tasks[kinds != 0]:
+        if kind == 1:
+            srcs = h["pair_src"][h["pair_ptr"][b]:h["pair_ptr"][e]] >> 6
+        else:
+            srcs = h["node_src"][h["node_ptr"][b]:h["node_ptr"][e]] >> 4
+        if srcs.size:
+            assert (srcs // granule).min() >= g - span_g - 1 and (srcs // granule).max() <= g
