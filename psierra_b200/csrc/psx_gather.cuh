@@ -2,9 +2,10 @@
 //
 // The element phase writes, per element e, a record into a ring of scratch slots
 // (slot = e & ring_mask):
-//   K part (KT): npair off-diagonal 3x3 blocks, 9 values each, oriented with rows = the
-//                element node of smaller global id; then npe diagonal blocks, 6 values
-//                each (xx xy xz yy yz zz).  npair = npe (npe - 1) / 2.
+//   K part (KT): npair off-diagonal 3x3 blocks, 12 values each (9 used, 16-byte
+//                aligned), oriented with rows = the element node of smaller global id;
+//                then npe diagonal blocks, 8 values each (xx xy xz yy yz zz + 2 pad).
+//                npair = npe (npe - 1) / 2.
 //   f part (double): 3 values per element node.
 // A pair item (i < j) sums the blocks of every element holding both nodes, in
 // ascending element order, and writes K_ij (row 3i+k, upper) and its transpose K_ji
@@ -21,10 +22,10 @@ namespace psx {
 template <int NPE>
 struct RecLayout {
   static constexpr int kPairs = NPE * (NPE - 1) / 2;
-  static constexpr int kK = kPairs * 9 + NPE * 6;  // KT values per element record
-  static constexpr int kF = NPE * 3;                // doubles per element f record
-  __host__ __device__ static constexpr int pair_off(int slot) { return slot * 9; }
-  __host__ __device__ static constexpr int diag_off(int a) { return kPairs * 9 + a * 6; }
+  static constexpr int kK = kPairs * 12 + NPE * 8;  // KT values per element record
+  static constexpr int kF = NPE * 3;                 // doubles per element f record
+  __host__ __device__ static constexpr int pair_off(int slot) { return slot * 12; }
+  __host__ __device__ static constexpr int diag_off(int a) { return kPairs * 12 + a * 8; }
 };
 
 struct GatherArgs {
@@ -39,13 +40,48 @@ struct GatherArgs {
   int64_t ring_mask;
 };
 
+// 16-byte vector loads/stores of record blocks (L2-only loads: the ring is rewritten while
+// the kernel runs, so nothing may be served from a stale L1 line).
 template <typename KT, int N>
-__device__ __forceinline__ void load_cg(const KT* __restrict__ p, KT v[N]) {
+__device__ __forceinline__ void load_block(const KT* __restrict__ p, KT v[N]) {
+  if constexpr (sizeof(KT) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
-  for (int i = 0; i < N; ++i) v[i] = __ldcg(p + i);
+    for (int i = 0; i < N / 4; ++i) {
+      const float4 t = __ldcg(q + i);
+      v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+    }
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const double2 t = __ldcg(q + i);
+      v[2 * i] = t.x; v[2 * i + 1] = t.y;
+    }
+  }
 }
 
-// Pair item: off-diagonal block and its transpose.
+template <typename KT, int N>
+__device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
+  if constexpr (sizeof(KT) == 4) {
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) __stcg(q + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+  } else {
+    double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) __stcg(q + i, make_double2(v[2 * i], v[2 * i + 1]));
+  }
+}
+
+// contributions whose loads are issued together (kept within the register budget)
+template <typename KT>
+struct Batch {
+  static constexpr int n = sizeof(KT) == 4 ? 4 : 2;
+};
+
+// Pair item: off-diagonal block and its transpose.  Contributions are summed in list
+// (ascending element) order; their loads are issued kBatch at a time.
 template <typename KT, int NPE>
 __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, const KT* __restrict__ krec,
                                             KT* __restrict__ k_out) {
@@ -55,21 +91,29 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
   KT acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = (KT)0;
-  for (int32_t s = s0; s < s1; ++s) {
-    const int32_t src = __ldg(g.pair_src + s);
-    const int64_t e = src >> 6;
-    const int slot = src & 63;
-    KT v[9];
-    load_cg<KT, 9>(krec + (e & g.ring_mask) * L::kK + L::pair_off(slot), v);
+  constexpr int kBatch = Batch<KT>::n;
+  for (int32_t s = s0; s < s1; s += kBatch) {
+    int32_t src[kBatch];
 #pragma unroll
-    for (int j = 0; j < 9; ++j) acc[j] += v[j];
+    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(g.pair_src + s + b) : -1;
+    KT v[kBatch][12];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (src[b] >= 0)
+        load_block<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * L::kK + L::pair_off(src[b] & 63), v[b]);
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (src[b] >= 0) {
+#pragma unroll
+        for (int j = 0; j < 9; ++j) acc[j] += v[b][j];
+      }
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      k_out[info.x + (int64_t)info.y * k + m] = acc[3 * k + m];
-      k_out[info.z + (int64_t)info.w * m + k] = acc[3 * k + m];
+      __stcs(k_out + info.x + (int64_t)info.y * k + m, acc[3 * k + m]);
+      __stcs(k_out + info.z + (int64_t)info.w * m + k, acc[3 * k + m]);
     }
 }
 
@@ -85,23 +129,39 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc[j] = (KT)0;
   double fa[3] = {0.0, 0.0, 0.0};
-  for (int32_t s = s0; s < s1; ++s) {
-    const int32_t src = __ldg(g.node_src + s);
-    const int64_t e = src >> 4;
-    const int a = src & 15;
-    const int64_t slot = e & g.ring_mask;
-    if constexpr (WANT_K) {
-      KT v[6];
-      load_cg<KT, 6>(krec + slot * L::kK + L::diag_off(a), v);
+  constexpr int kBatch = Batch<KT>::n;
+  for (int32_t s = s0; s < s1; s += kBatch) {
+    int32_t src[kBatch];
 #pragma unroll
-      for (int j = 0; j < 6; ++j) acc[j] += v[j];
-    }
-    if constexpr (WANT_F) {
-      const double* fp = frec + slot * L::kF + 3 * a;
-      fa[0] += __ldcg(fp);
-      fa[1] += __ldcg(fp + 1);
-      fa[2] += __ldcg(fp + 2);
-    }
+    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(g.node_src + s + b) : -1;
+    KT v[kBatch][8];
+    double fv[kBatch][3];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (src[b] >= 0) {
+        const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;
+        const int a = src[b] & 15;
+        if constexpr (WANT_K) load_block<KT, 8>(krec + slot * L::kK + L::diag_off(a), v[b]);
+        if constexpr (WANT_F) {
+          const double* fp = frec + slot * L::kF + 3 * a;
+          fv[b][0] = __ldcg(fp);
+          fv[b][1] = __ldcg(fp + 1);
+          fv[b][2] = __ldcg(fp + 2);
+        }
+      }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (src[b] >= 0) {
+        if constexpr (WANT_K) {
+#pragma unroll
+          for (int j = 0; j < 6; ++j) acc[j] += v[b][j];
+        }
+        if constexpr (WANT_F) {
+          fa[0] += fv[b][0];
+          fa[1] += fv[b][1];
+          fa[2] += fv[b][2];
+        }
+      }
   }
   if constexpr (WANT_K) {
     if (info.y > 0) {
@@ -109,35 +169,39 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[info.x + (int64_t)info.y * k + m] = full[3 * k + m];
+        for (int m = 0; m < 3; ++m) __stcs(k_out + info.x + (int64_t)info.y * k + m, full[3 * k + m]);
     }
   }
   if constexpr (WANT_F) {
-    f_out[3 * (int64_t)info.z + 0] = fa[0];
-    f_out[3 * (int64_t)info.z + 1] = fa[1];
-    f_out[3 * (int64_t)info.z + 2] = fa[2];
+    __stcs(f_out + 3 * (int64_t)info.z + 0, fa[0]);
+    __stcs(f_out + 3 * (int64_t)info.z + 1, fa[1]);
+    __stcs(f_out + 3 * (int64_t)info.z + 2, fa[2]);
   }
 }
 
-// Store an off-diagonal block record (9 values), transposed when `swap`.
+// Store an off-diagonal block record (9 values + 3 pad), transposed when `swap`.
 template <typename KT>
 __device__ __forceinline__ void store_pair_block(KT* __restrict__ dst, const KT b[9], bool swap) {
+  KT o[12];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
-    for (int m = 0; m < 3; ++m) __stcg(dst + 3 * k + m, swap ? b[3 * m + k] : b[3 * k + m]);
+    for (int m = 0; m < 3; ++m) o[3 * k + m] = swap ? b[3 * m + k] : b[3 * k + m];
+  o[9] = o[10] = o[11] = (KT)0;
+  store_block<KT, 12>(dst, o);
 }
 
-// Store a diagonal block record: xx xy xz yy yz zz.
+// Store a diagonal block record: xx xy xz yy yz zz (+2 pad).
 template <typename KT>
 __device__ __forceinline__ void store_diag_block(KT* __restrict__ dst, const KT d[6]) {
-#pragma unroll
-  for (int i = 0; i < 6; ++i) __stcg(dst + i, d[i]);
+  const KT o[8] = {d[0], d[1], d[2], d[3], d[4], d[5], (KT)0, (KT)0};
+  store_block<KT, 8>(dst, o);
 }
 
 // ---- persistent task queue --------------------------------------------------------
-// Counters live at the start of the workspace: [0] next task, [1 .. G] element tiles
-// finished per granule, [1 + G .. 2G] gather tiles finished per granule.
+// Tasks are claimed by warps (32 elements or 32 items each).  Counters live at the
+// start of the workspace: [0] next task, [1 .. G] element tiles finished per granule,
+// [1 + G .. 2G] gather tiles finished per granule.
 struct QueueArgs {
   const int4* tasks;
   int32_t n_tasks;
@@ -157,7 +221,7 @@ __device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
   return v;
 }
 
-// Bounded wait, executed by warp 0 of the block: lane j checks counter[first + j] >=
+// Bounded wait, executed by a whole warp: lane j checks counter[first + j] >=
 // target(first + j) for j < count.  Returns false (and flags the status) if the wait
 // gives up; the caller then still proceeds, so every access stays in bounds and the
 // host reports the failure.
@@ -211,7 +275,7 @@ inline int32_t device_sm_count() {
 // ring of f records (each 256-byte aligned).  The ring spans a power-of-two number of
 // granules covering the item span plus the blocks in flight; with `work` null only the
 // sizes are computed.
-inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayout* W) {
+inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayout* W, int blocks_per_sm = 3) {
   if (!P || !W || P->n_elements <= 0 || P->n_nodes <= 0 || P->granule <= 0 || (P->granule & (P->granule - 1)))
     return PSX_ERR_ARG;
   if (!P->conn || !P->pair_info || !P->pair_ptr || !P->pair_src || !P->node_info || !P->node_ptr ||
@@ -229,13 +293,13 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   int32_t all = 1;
   while (all < P->n_granules) all <<= 1;
   int32_t ring = 1;
-  while (ring < W->span_g + 12) ring <<= 1;
+  while (ring < W->span_g + 6) ring <<= 1;
   W->ring_g = ring < all ? ring : all;
   W->ring_elems = (int64_t)W->ring_g * P->granule;
   const int sms = device_sm_count();
   if (sms <= 0) return PSX_ERR_CUDA;
   const int64_t ntask = P->n_tasks_k > P->n_tasks_f ? P->n_tasks_k : P->n_tasks_f;
-  W->grid = (int32_t)(sms * 4 < ntask ? sms * 4 : ntask);
+  W->grid = (int32_t)(sms * blocks_per_sm < ntask ? sms * blocks_per_sm : ntask);
   auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
   W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
   const int64_t kbytes = up(W->ring_elems * kK * kt);

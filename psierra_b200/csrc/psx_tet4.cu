@@ -28,6 +28,10 @@ namespace psx {
 namespace {
 
 constexpr int kThreads = 128;
+#ifndef PSX_TET4_MIN_BLOCKS
+#define PSX_TET4_MIN_BLOCKS 3
+#endif
+constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the register budget targets
 
 struct Tet4Geom {
   double g[4][3];  // shape-function gradients
@@ -195,19 +199,20 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   }
 }
 
-// Persistent assembly kernel: each block repeatedly claims the next task of the queue
+// Persistent assembly kernel: each warp repeatedly claims the next task of the queue
 // (psx_task_fill).  Element tiles publish their granule's completion count; gather
 // tiles wait for the element granules they read; element tiles wait until the gather
 // tiles still reading the ring slots they overwrite are done.  Every wait is on tasks
-// that earlier blocks have already claimed, so the queue always drains.
+// that earlier warps have already claimed, so the queue always drains.  There are no
+// block-wide barriers: warps of a block progress independently.
 template <typename KT, int MODE>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
                        KT* __restrict__ k_out, double* __restrict__ f_out) {
   using L = RecLayout<4>;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
-  __shared__ int4 s_task;
+  const int lane = threadIdx.x & 31;
   int32_t* acnt = Q.counters + 1;
   int32_t* bcnt = Q.counters + 1 + Q.n_granules;
   const int64_t gsize = (int64_t)1 << Q.granule_log2;
@@ -217,37 +222,29 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
   };
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
   while (true) {
-    if (threadIdx.x == 0) {
-      const int32_t t = atomicAdd(Q.counters, 1);
-      s_task = t < Q.n_tasks ? __ldg(Q.tasks + t) : make_int4(-1, 0, 0, 0);
-    }
-    __syncthreads();
-    const int4 task = s_task;
-    __syncthreads();
-    if (task.x < 0) break;
+    int32_t t = 0;
+    if (lane == 0) t = atomicAdd(Q.counters, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= Q.n_tasks) break;
+    const int4 task = __ldg(Q.tasks + t);
     const int32_t gr = task.y;
     if (task.x == 0) {
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0 && threadIdx.x < 32) {
-        const int32_t cnt = min(Q.span_g + 2, Q.n_granules - old);
-        wait_counters(bcnt, old, cnt, btiles, A.st);
-      }
-      __syncthreads();
-      const int64_t e = task.z + (int64_t)threadIdx.x;
+      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, A.st);
+      __syncwarp();
+      const int64_t e = task.z + (int64_t)lane;
       if (e < task.w) {
         const int64_t slot = e & g.ring_mask;
         tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
       }
       __threadfence();
-      __syncthreads();
-      if (threadIdx.x == 0) atomicAdd(acnt + gr, 1);
+      __syncwarp();
+      if (lane == 0) atomicAdd(acnt + gr, 1);
     } else {
-      if (threadIdx.x < 32) {
-        const int32_t first = max(0, gr - Q.span_g - 1);
-        wait_counters(acnt, first, gr - first + 1, atiles, A.st);
-      }
-      __syncthreads();
-      const int32_t item = task.z + threadIdx.x;
+      const int32_t first = max(0, gr - Q.span_g - 1);
+      wait_counters(acnt, first, gr - first + 1, atiles, A.st);
+      __syncwarp();
+      const int32_t item = task.z + lane;
       if (item < task.w) {
         if (task.x == 1) {
           gather_pair<KT, 4>(g, item, krec, k_out);
@@ -255,9 +252,8 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
           gather_node<KT, 4, kWantK, kWantF>(g, item, krec, frec, k_out, f_out);
         }
       }
-      __threadfence();
-      __syncthreads();
-      if (threadIdx.x == 0) atomicAdd(bcnt + gr, 1);
+      __syncwarp();
+      if (lane == 0) atomicAdd(bcnt + gr, 1);
     }
   }
 }

@@ -65,7 +65,7 @@ class MeshPattern:
         return self._blocks
 
     GRANULE = 4096
-    TILE = 128
+    TILE = 32
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
