@@ -54,7 +54,8 @@ extern "C" {
  * Status block written by the element kernels (device memory, psx_status_bytes()
  * bytes, zero it before a call).  Layout: int32 n_inverted, int32 n_bad_volume,
  * int32 first_bad_key (INT32_MAX - lowest bad element index, 0 if none),
- * int32 n_not_finite, int32 iters, int32 flags, double value.
+ * int32 n_not_finite, int32 iters, int32 flags, double value.  The assembly kernels
+ * put the number of spin iterations of their bounded waits in `iters`.
  * An element is "bad" when its reference volume det is <= 0 (n_bad_volume) or
  * det F <= 0 (n_inverted): the two conditions on which the reference raises
  * ValueError (element/tet4_base.py:56-61, element/tet4_total_lagrangian.py:110-112).
@@ -132,7 +133,7 @@ typedef struct psx_plan {
   const int32_t* pair_gptr; /* host, n_granules + 1: pair items ready in each granule */
   const int32_t* node_gptr; /* host, n_granules + 1 */
   int32_t tile;             /* items per task (psx_task_fill) */
-  int32_t pad_;
+  int32_t lag;              /* granules between an element tile and the gathers it completes */
   int64_t n_tasks_k;        /* task queue with pair tiles (any request involving K) */
   int64_t n_tasks_f;        /* task queue without pair tiles (f only) */
   const int32_t* tasks_k;   /* device, 4 per task: kind, granule, begin, end */
@@ -158,13 +159,13 @@ int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int3
 
 /*
  * Task queue of the persistent assembly kernel (host): for each granule g, the
- * element tiles of g followed by the gather tiles made ready by granule g-1 (pairs
- * when with_pairs, then nodes).  Each task is 4 int32 {kind, granule, begin, end};
+ * element tiles of g followed by the gather tiles made ready by granule g-1-lag
+ * (pairs when with_pairs, then nodes).  Each task is 4 int32 {kind, granule, begin, end};
  * b_tiles_per_granule (n_granules) counts the gather tiles of each granule.  `tile` must
  * divide the plan granule.  Uses only the host fields of `plan`.
  */
-int psx_task_count(const psx_plan_t* plan, int with_pairs, int32_t tile, int64_t* n_tasks);
-int psx_task_fill(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t* tasks,
+int psx_task_count(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t lag, int64_t* n_tasks);
+int psx_task_fill(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t lag, int32_t* tasks,
                   int32_t* b_tiles_per_granule);
 
 /*

@@ -42,8 +42,8 @@ SIGNATURES: dict[str, list] = {
     "psx_block_lists": [_p, _i64, _i32, _i64, _p, _p, _p, _p],
     "psx_plan_count": [_p, _i64, _i32, _i64, _p, _p, _p],
     "psx_plan_fill": [_p, _i64, _i32, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _p, _p, _p],
-    "psx_task_count": [_p, _i32, _i32, _p],
-    "psx_task_fill": [_p, _i32, _i32, _p, _p],
+    "psx_task_count": [_p, _i32, _i32, _i32, _p],
+    "psx_task_fill": [_p, _i32, _i32, _i32, _p, _p],
     "psx_work_bytes": [_p, _i32, _p, _p],
     "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _p, _p, _p, _i64, _p, _p],
     "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
@@ -72,7 +72,7 @@ class PlanStruct(ctypes.Structure):
         ("pair_gptr", ctypes.c_void_p),
         ("node_gptr", ctypes.c_void_p),
         ("tile", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("lag", ctypes.c_int32),
         ("n_tasks_k", ctypes.c_int64),
         ("n_tasks_f", ctypes.c_int64),
         ("tasks_k", ctypes.c_void_p),

@@ -162,6 +162,10 @@ class GPUAssembler:
         first = int(0x7FFFFFFF - int(s[2])) if s[2] != 0 else -1
         return int(s[0]), int(s[1]), first, int(s[5])
 
+    def last_spins(self) -> int:
+        """Spin iterations the bounded waits of the last sweep took (synchronises)."""
+        return int(self.status[4].item())
+
     def raise_on_bad_elements(self, u: torch.Tensor | None) -> None:
         n_inv, n_vol, first, flags = self.status_counts()
         if flags & 1:

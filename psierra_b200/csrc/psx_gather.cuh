@@ -245,6 +245,7 @@ __device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first,
       }
       if (spins > 64) __nanosleep(200);
     }
+    if (spins && lane == 0) atomicAdd(&st->iters, spins);
   }
   return true;
 }
@@ -293,7 +294,7 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   int32_t all = 1;
   while (all < P->n_granules) all <<= 1;
   int32_t ring = 1;
-  while (ring < W->span_g + 6) ring <<= 1;
+  while (ring < W->span_g + P->lag + 6) ring <<= 1;
   W->ring_g = ring < all ? ring : all;
   W->ring_elems = (int64_t)W->ring_g * P->granule;
   const int sms = device_sm_count();

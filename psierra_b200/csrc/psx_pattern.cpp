@@ -316,21 +316,23 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
 
 // ---------------------------------------------------------------------------
 // Task queue of the persistent assembly kernel: for each granule g, the element
-// tiles of g followed by the gather tiles made ready by granule g-1 (pairs, then
-// nodes); the gather tiles of the last granule close the queue.  Task = int4
+// tiles of g followed by the gather tiles made ready by granule g-1-lag (pairs, then
+// nodes); the gather tiles of the last granules close the queue.  The lag keeps gather
+// tiles from being claimed while the element tiles they read are still running.  Task = int4
 // {kind, granule, begin, end}: kind 0 = element tile [begin, end), 1 = pair items,
 // 2 = node items.  `with_pairs` = 0 builds the f-only queue (no pair tiles).
-extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile, int64_t* n_tasks) {
-  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || !n_tasks) return PSX_ERR_ARG;
+extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t lag, int64_t* n_tasks) {
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || lag < 0 || !n_tasks)
+    return PSX_ERR_ARG;
   int64_t n = 0;
   const int64_t G = P->n_granules;
-  for (int64_t g = 0; g <= G; ++g) {
+  for (int64_t g = 0; g <= G + lag; ++g) {
     if (g < G) {
       const int64_t e0 = g * P->granule, e1 = std::min<int64_t>(P->n_elements, e0 + P->granule);
       n += (e1 - e0 + tile - 1) / tile;
     }
-    if (g >= 1) {
-      const int64_t r = g - 1;
+    if (g >= 1 + lag && g - 1 - lag < G) {
+      const int64_t r = g - 1 - lag;
       if (with_pairs) n += (P->pair_gptr[r + 1] - P->pair_gptr[r] + tile - 1) / tile;
       const int64_t n0 = r == 0 ? 0 : P->node_gptr[r];
       n += (P->node_gptr[r + 1] - n0 + tile - 1) / tile;
@@ -340,9 +342,10 @@ extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile,
   return PSX_OK;
 }
 
-extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t* tasks,
+extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t lag, int32_t* tasks,
                              int32_t* b_tiles_per_granule) {
-  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || !tasks || !b_tiles_per_granule)
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || lag < 0 || !tasks ||
+      !b_tiles_per_granule)
     return PSX_ERR_ARG;
   const int64_t G = P->n_granules;
   int64_t k = 0;
@@ -353,13 +356,13 @@ extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, 
     tasks[4 * k + 3] = (int32_t)e;
     ++k;
   };
-  for (int64_t g = 0; g <= G; ++g) {
+  for (int64_t g = 0; g <= G + lag; ++g) {
     if (g < G) {
       const int64_t e0 = g * P->granule, e1 = std::min<int64_t>(P->n_elements, e0 + P->granule);
       for (int64_t b = e0; b < e1; b += tile) push(0, g, b, std::min<int64_t>(e1, b + tile));
     }
-    if (g >= 1) {
-      const int64_t r = g - 1;
+    if (g >= 1 + lag && g - 1 - lag < G) {
+      const int64_t r = g - 1 - lag;
       int32_t nb = 0;
       if (with_pairs)
         for (int64_t b = P->pair_gptr[r]; b < P->pair_gptr[r + 1]; b += tile, ++nb)

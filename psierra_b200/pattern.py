@@ -66,6 +66,7 @@ class MeshPattern:
 
     GRANULE = 4096
     TILE = 32
+    LAG = 4
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
@@ -124,14 +125,15 @@ class MeshPattern:
                 setattr(st, k, d[k].data_ptr())
             st.pair_gptr = h["pair_gptr"].ctypes.data
             st.node_gptr = h["node_gptr"].ctypes.data
-            st.tile = self.TILE
+            st.tile, st.lag = self.TILE, self.LAG
             L = lib()
             for key, with_pairs in (("k", 1), ("f", 0)):
                 nt = ctypes.c_int64()
-                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.TILE, ctypes.byref(nt)), "psx_task_count")
+                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.TILE, self.LAG, ctypes.byref(nt)),
+                      "psx_task_count")
                 tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
                 btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
-                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.TILE, ptr(tasks), ptr(btiles)),
+                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.TILE, self.LAG, ptr(tasks), ptr(btiles)),
                       "psx_task_fill")
                 d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
                 setattr(st, "n_tasks_" + key, int(nt.value))

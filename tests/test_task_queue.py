@@ -1,6 +1,7 @@
 """Deadlock freedom and ring safety of the persistent assembly kernel's task queue (CPU).
 
 The kernel's wait rules, restated:
+* gather tiles of granule r are queued after the element tiles of granule r + 1 + lag;
 * an element tile of granule g waits for all gather tiles of granules
   [g - R, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
   slots of granule g - R, if g - R >= 0;
@@ -20,7 +21,7 @@ from psierra_b200 import _lib, meshgen
 from psierra_b200.pattern import MeshPattern
 
 
-def _queue(p: MeshPattern, with_pairs: int, tile: int):
+def _queue(p: MeshPattern, with_pairs: int, tile: int, lag: int):
     h = p.plan_host()
     st = _lib.PlanStruct()
     st.npe, st.n_granules = p.npe, h["n_granules"]
@@ -29,20 +30,21 @@ def _queue(p: MeshPattern, with_pairs: int, tile: int):
     st.pair_gptr, st.node_gptr = h["pair_gptr"].ctypes.data, h["node_gptr"].ctypes.data
     L = _lib.lib()
     nt = ctypes.c_int64()
-    _lib.check(L.psx_task_count(ctypes.byref(st), with_pairs, tile, ctypes.byref(nt)), "count")
+    _lib.check(L.psx_task_count(ctypes.byref(st), with_pairs, tile, lag, ctypes.byref(nt)), "count")
     tasks = np.zeros(4 * nt.value, dtype=np.int32)
     bt = np.zeros(h["n_granules"], dtype=np.int32)
-    _lib.check(L.psx_task_fill(ctypes.byref(st), with_pairs, tile, _lib.ptr(tasks), _lib.ptr(bt)), "fill")
+    _lib.check(L.psx_task_fill(ctypes.byref(st), with_pairs, tile, lag, _lib.ptr(tasks), _lib.ptr(bt)), "fill")
     return tasks.reshape(-1, 4), bt, h
 
 
-@pytest.mark.parametrize("granule,with_pairs", [(256, 1), (256, 0), (512, 1), (128, 1)])
-def test_waits_only_on_earlier_tasks(granule, with_pairs):
+@pytest.mark.parametrize("granule,with_pairs,lag", [(256, 1, 0), (256, 0, 4), (512, 1, 4), (128, 1, 2),
+                                                    (128, 1, 7)])
+def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
     m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
     p = MeshPattern(m.elements, m.n_nodes)
     p.GRANULE = granule
     tile = 64
-    tasks, bt, h = _queue(p, with_pairs, tile)
+    tasks, bt, h = _queue(p, with_pairs, tile, lag)
     G = h["n_granules"]
     span_g = -(-int(h["max_span"][0]) // granule)
     # all items covered exactly once
@@ -54,9 +56,9 @@ def test_waits_only_on_earlier_tasks(granule, with_pairs):
     # gather tile counts per granule match
     for r in range(G):
         assert bt[r] == np.count_nonzero((kinds != 0) & (tasks[:, 1] == r))
-    # the kernel's ring length (power of two >= span_g + 12, capped to cover all granules)
+    # the kernel's ring length (power of two >= span_g + lag + 6, capped to cover all granules)
     all_g = 1 << int(np.ceil(np.log2(max(G, 1))))
-    ring = 1 << int(np.ceil(np.log2(span_g + 12)))
+    ring = 1 << int(np.ceil(np.log2(span_g + lag + 6)))
     ring = min(ring, all_g)
     last_a = {}
     last_b = {}
