@@ -9,7 +9,7 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libpsierra_b200.so")
+LIB_PATH = os.environ.get("PSIERRA_B200_LIB") or os.path.join(_HERE, "libpsierra_b200.so")
 
 PSX_OK = 0
 PSX_ERR_ARG = 1

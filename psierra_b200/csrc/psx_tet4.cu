@@ -221,31 +221,33 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
     return (int32_t)((n + Q.tile - 1) / Q.tile);
   };
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  // the claim of the next task is issued before the current one is worked on
+  int32_t next = 0;
+  if (lane == 0) next = atomicAdd(Q.counters, 1);
   while (true) {
-    int32_t t = 0;
-    if (lane == 0) t = atomicAdd(Q.counters, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
+    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
     if (t >= Q.n_tasks) break;
+    if (lane == 0) next = atomicAdd(Q.counters, 1);
     const int4 task = __ldg(Q.tasks + t);
     const int32_t gr = task.y;
     if (task.x == 0) {
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
       if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, A.st);
       __syncwarp();
-      const int64_t e = task.z + (int64_t)lane;
-      if (e < task.w) {
+      for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
         const int64_t slot = e & g.ring_mask;
         tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
       }
-      __threadfence();
       __syncwarp();
-      if (lane == 0) atomicAdd(acnt + gr, 1);
+      if (lane == 0) {
+        __threadfence();
+        atomicAdd(acnt + gr, 1);
+      }
     } else {
       const int32_t first = max(0, gr - Q.span_g - 1);
       wait_counters(acnt, first, gr - first + 1, atiles, A.st);
       __syncwarp();
-      const int32_t item = task.z + lane;
-      if (item < task.w) {
+      for (int32_t item = task.z + lane; item < task.w; item += 32) {
         if (task.x == 1) {
           gather_pair<KT, 4>(g, item, krec, k_out);
         } else {
@@ -338,7 +340,7 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   if (wantF && !f_out) return PSX_ERR_ARG;
   if (wantK && !k_out) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, precision, work, &W);
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};

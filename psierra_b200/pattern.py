@@ -65,8 +65,8 @@ class MeshPattern:
         return self._blocks
 
     GRANULE = 4096
-    TILE = 32
-    LAG = 4
+    TILE = 128
+    LAG = 8
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
