@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kThreads = 128;
 #ifndef PSX_TET4_MIN_BLOCKS
-#define PSX_TET4_MIN_BLOCKS 3
+#define PSX_TET4_MIN_BLOCKS 2
 #endif
 constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the register budget targets
 

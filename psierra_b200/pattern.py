@@ -65,7 +65,7 @@ class MeshPattern:
         return self._blocks
 
     GRANULE = 4096
-    TILE = 128
+    TILE = 32
     LAG = 8
 
     def plan_host(self) -> dict:
