@@ -165,9 +165,9 @@ extern "C" int psx_block_lists(const int64_t* conn, int64_t E, int npe, int64_t 
 // Items: every node pair (i < j) of the node graph ("pair", off-diagonal block K_ij and
 // its transpose K_ji) and every node ("node", diagonal block K_ii and f_i).  Each item
 // lists its contributing element slots in ascending element order; items are sorted by
-// their "ready" element (the largest contributing element id), so that the items
-// completed by an element range [0, c) form a prefix, and granule ranges of the sorted
-// item lists can be gathered right after that element range has been evaluated.
+// the granule of their "ready" element (the largest contributing element id) and keep
+// their (i, j) order inside a granule, so that the items completed by granules [0, g)
+// form a prefix and can be gathered right after those elements have been evaluated.
 namespace {
 
 inline int local_pair_index(int a, int b, int npe) {  // a < b
@@ -266,8 +266,15 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
   auto by_ready = [](const Item& x, const Item& y) {
     return x.ready < y.ready || (x.ready == y.ready && x.order < y.order);
   };
-  std::sort(p_item.begin(), p_item.end(), by_ready);
-  std::sort(n_item.begin(), n_item.end(), by_ready);
+  // Within a granule, items keep (i, j) order (their original order), so that lanes of a
+  // gather tile write neighbouring blocks of the same CSR rows.
+  auto by_granule = [granule](const Item& x, const Item& y) {
+    const int64_t gx = x.ready < 0 ? -1 : x.ready / granule, gy = y.ready < 0 ? -1 : y.ready / granule;
+    return gx < gy || (gx == gy && x.order < y.order);
+  };
+  std::sort(p_item.begin(), p_item.end(), by_granule);
+  std::sort(n_item.begin(), n_item.end(), by_granule);
+  (void)by_ready;
 
   // ---- emit pairs in ready order
   int32_t out = 0;

@@ -205,6 +205,16 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 // tiles still reading the ring slots they overwrite are done.  Every wait is on tasks
 // that earlier warps have already claimed, so the queue always drains.  There are no
 // block-wide barriers: warps of a block progress independently.
+// Records of a warp's 32 consecutive elements are staged in shared memory (FP32) and
+// copied to the ring as one contiguous block, so the ring sees whole-sector writes.
+constexpr int kStageStride = RecLayout<4>::kK + 4;  // floats per staged record (bank spread)
+
+template <typename KT>
+struct StageSmem {
+  static constexpr bool kOn = sizeof(KT) == 4;
+  static constexpr int kWarpFloats = kOn ? 32 * kStageStride : 1;
+};
+
 template <typename KT, int MODE>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
@@ -221,6 +231,9 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
     return (int32_t)((n + Q.tile - 1) / Q.tile);
   };
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
+  extern __shared__ __align__(16) float s_stage[];  // kThreads/32 warps x kWarpFloats (FP32 K only)
+  float* my_stage = s_stage + (threadIdx.x >> 5) * StageSmem<KT>::kWarpFloats;
   // the claim of the next task is issued before the current one is worked on
   int32_t next = 0;
   if (lane == 0) next = atomicAdd(Q.counters, 1);
@@ -234,11 +247,29 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
       if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, A.st);
       __syncwarp();
-      for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
-        const int64_t slot = e & g.ring_mask;
-        tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
+      if constexpr (kStage) {
+        // tiles are 32 consecutive elements inside one granule: their ring slots are contiguous
+        const int64_t e = task.z + (int64_t)lane;
+        const int64_t slot0 = (int64_t)task.z & g.ring_mask;
+        if (e < task.w)
+          tet4_element<KT, MODE>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
+                                 frec + (e & g.ring_mask) * L::kF);
+        __syncwarp();
+        const int n = task.w - task.z;
+        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(krec) + slot0 * L::kK);
+        constexpr int kChunks = L::kK / 4;  // float4 per record
+        for (int c = lane; c < n * kChunks; c += 32) {
+          const int el = c / kChunks, q = c - el * kChunks;
+          __stcg(dst + c, *reinterpret_cast<const float4*>(my_stage + el * kStageStride + 4 * q));
+        }
+        __syncwarp();
+      } else {
+        for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
+          const int64_t slot = e & g.ring_mask;
+          tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
+        }
+        __syncwarp();
       }
-      __syncwarp();
       if (lane == 0) {
         __threadfence();
         atomicAdd(acnt + gr, 1);
@@ -306,8 +337,14 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   Q.ring_g = W.ring_g;
   Q.n_elements = P->n_elements;
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
-  tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, 0, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
-                                                                   k_out, f_out);
+  constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
+  const size_t smem = kStage ? sizeof(float) * (kThreads / 32) * StageSmem<KT>::kWarpFloats : 0;
+  if (smem > 0 &&
+      cudaFuncSetAttribute(tet4_persistent_kernel<KT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return PSX_ERR_CUDA;
+  tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
+                                                                      k_out, f_out);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }
