@@ -61,9 +61,14 @@ __device__ __forceinline__ void load_block(const KT* __restrict__ p, KT v[N]) {
   }
 }
 
-template <typename KT, int N>
+// GLOBAL: `p` is global memory (L2-only store); otherwise a plain store through a
+// generic pointer (used for the shared-memory staging of records).
+template <typename KT, int N, bool GLOBAL = true>
 __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
-  if constexpr (sizeof(KT) == 4) {
+  if constexpr (!GLOBAL) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) p[i] = v[i];
+  } else if constexpr (sizeof(KT) == 4) {
     float4* q = reinterpret_cast<float4*>(p);
 #pragma unroll
     for (int i = 0; i < N / 4; ++i) __stcg(q + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
@@ -180,7 +185,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 }
 
 // Store an off-diagonal block record (9 values + 3 pad), transposed when `swap`.
-template <typename KT>
+template <typename KT, bool GLOBAL = true>
 __device__ __forceinline__ void store_pair_block(KT* __restrict__ dst, const KT b[9], bool swap) {
   KT o[12];
 #pragma unroll
@@ -188,14 +193,14 @@ __device__ __forceinline__ void store_pair_block(KT* __restrict__ dst, const KT 
 #pragma unroll
     for (int m = 0; m < 3; ++m) o[3 * k + m] = swap ? b[3 * m + k] : b[3 * k + m];
   o[9] = o[10] = o[11] = (KT)0;
-  store_block<KT, 12>(dst, o);
+  store_block<KT, 12, GLOBAL>(dst, o);
 }
 
 // Store a diagonal block record: xx xy xz yy yz zz (+2 pad).
-template <typename KT>
+template <typename KT, bool GLOBAL = true>
 __device__ __forceinline__ void store_diag_block(KT* __restrict__ dst, const KT d[6]) {
   const KT o[8] = {d[0], d[1], d[2], d[3], d[4], d[5], (KT)0, (KT)0};
-  store_block<KT, 8>(dst, o);
+  store_block<KT, 8, GLOBAL>(dst, o);
 }
 
 // ---- persistent task queue --------------------------------------------------------

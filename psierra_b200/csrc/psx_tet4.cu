@@ -94,7 +94,9 @@ struct Tet4Args {
 
 // Phase A: one element -> its record.  tet4_total_lagrangian.py:77-139 (and, with
 // PSX_LINEAR, tet4_base.py:129-136) in the closed form of psx_common.cuh.
-template <typename KT, int MODE>
+// `krec` is global memory when KGLOBAL, else the shared-memory staging slot of the lane;
+// `frec` is always global memory.
+template <typename KT, int MODE, bool KGLOBAL = true>
 __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
                                              double* __restrict__ frec) {
   using L = RecLayout<4>;
@@ -189,9 +191,9 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
             v[3 * k + m] = p[a][k] * w[b][m] + p[b][k] * h[a][m] + y[a][k] * p[b][m] + (k == m ? s : (KT)0);
         if (b == a) {
           const KT d[6] = {v[0], v[1], v[2], v[4], v[5], v[8]};
-          store_diag_block<KT>(krec + L::diag_off(a), d);
+          store_diag_block<KT, KGLOBAL>(krec + L::diag_off(a), d);
         } else {
-          store_pair_block<KT>(krec + L::pair_off(slot), v, gid[a] > gid[b]);
+          store_pair_block<KT, KGLOBAL>(krec + L::pair_off(slot), v, gid[a] > gid[b]);
           ++slot;
         }
       }
@@ -252,8 +254,8 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
         const int64_t e = task.z + (int64_t)lane;
         const int64_t slot0 = (int64_t)task.z & g.ring_mask;
         if (e < task.w)
-          tet4_element<KT, MODE>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
-                                 frec + (e & g.ring_mask) * L::kF);
+          tet4_element<KT, MODE, false>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
+                                        frec + (e & g.ring_mask) * L::kF);
         __syncwarp();
         const int n = task.w - task.z;
         float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(krec) + slot0 * L::kK);
