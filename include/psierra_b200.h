@@ -45,6 +45,7 @@ extern "C" {
 #define PSX_WANT_F 1            /* internal force vector f_int(u) */
 #define PSX_WANT_K 2            /* tangent stiffness K_T(u) values in the CSR pattern */
 #define PSX_LINEAR 4            /* small-strain stiffness from (lambda, mu); ignores u */
+#define PSX_KV 8                /* matrix-free product y = K_T(u) v (psx_tet4_kv) */
 
 /* Precision of the element tangent (`precision`) */
 #define PSX_FP64 0              /* everything in FP64, K values stored as double */
@@ -195,6 +196,31 @@ int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u,
                       const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,
                       int mode, int precision, double* f_out, void* k_out, void* work,
                       int64_t work_bytes, void* status, void* stream);
+
+/*
+ * Matrix-free tangent product y = K_T(u) v (no matrix is formed): each element
+ * evaluates K_e v_e from its kinematics in closed form and the node gather sums the
+ * contributions in fixed order, so y equals the assembled K_T @ v of the reference
+ * (domain/solid.py:280-325 followed by a CSR product) to rounding.
+ *   v, y_out (device, 3N doubles); work as for psx_tet4_assemble.
+ */
+int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double* u,
+                const double* mu_e, const double* kappa_e, double mu, double kappa, int precision,
+                const double* v, double* y_out, void* work, int64_t work_bytes, void* status,
+                void* stream);
+
+/*
+ * One dynamic-relaxation pseudo-step on the linearised system K_T(u) x = b, fused into
+ * a single pass (the viscous update of analysis/dynamic_relaxation.py:296-299,378-382):
+ *   r = b - K_T(u) x,  a = minv * r,  vel = c1 vel + c2 a,  x += dt vel   (in place)
+ * minv (device, 3N) is the inverse lumped mass, 0 on prescribed DOFs; r_out (device,
+ * 3N, optional) receives the residual r of the incoming x.
+ */
+int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const double* u,
+                     const double* mu_e, const double* kappa_e, double mu, double kappa, int precision,
+                     const double* b, const double* minv, double c1, double c2, double dt,
+                     double* x, double* vel, double* r_out, void* work, int64_t work_bytes,
+                     void* status, void* stream);
 
 /*
  * Reference det (of [1 X], = 6 V) and det F of one element, written to out2

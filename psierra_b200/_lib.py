@@ -19,6 +19,7 @@ PSX_ERR_LIMIT = 3
 PSX_WANT_F = 1
 PSX_WANT_K = 2
 PSX_LINEAR = 4
+PSX_KV = 8
 
 PSX_FP64 = 0
 PSX_FP32_MIXED = 1
@@ -46,6 +47,9 @@ SIGNATURES: dict[str, list] = {
     "psx_task_fill": [_p, _i32, _i32, _i32, _p, _p],
     "psx_work_bytes": [_p, _i32, _p, _p],
     "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _p, _p, _p, _i64, _p, _p],
+    "psx_tet4_kv": [_p, _p, _p, _p, _p, _f64, _f64, _i32, _p, _p, _p, _i64, _p, _p],
+    "psx_tet4_dr_step": [_p, _p, _p, _p, _p, _f64, _f64, _i32, _p, _p, _f64, _f64, _f64, _p, _p, _p, _p, _i64,
+                         _p, _p],
     "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
 }
 

@@ -148,6 +148,37 @@ class GPUAssembler:
             self.raise_on_bad_elements(u)
         return (f_out if want_f else None), (k_out if want_k else None)
 
+    def kv(self, u: torch.Tensor, v: torch.Tensor, precision: str | None = None,
+           y_out: torch.Tensor | None = None, check_status: bool = True) -> torch.Tensor:
+        """Matrix-free ``y = K_T(u) v`` (float64 in and out; element math in ``precision``)."""
+        prec = precision or self.precision
+        u = self._check_u(u)
+        v = self._check_u(v)
+        if y_out is None:
+            y_out = self.new_f()
+        self.status.zero_()
+        work = self.workspace(prec)
+        check(lib().psx_tet4_kv(ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u), ptr(self.mu_e),
+                                ptr(self.kappa_e), self.mu, self.kappa, PRECISIONS[prec], ptr(v), ptr(y_out),
+                                ptr(work), work.numel(), ptr(self.status), _stream_handle()), "psx_tet4_kv")
+        if check_status:
+            self.raise_on_bad_elements(u)
+        return y_out
+
+    def dr_step(self, u: torch.Tensor, b: torch.Tensor, minv: torch.Tensor, x: torch.Tensor, vel: torch.Tensor,
+                c1: float, c2: float, dt: float, precision: str | None = None,
+                r_out: torch.Tensor | None = None) -> None:
+        """One fused dynamic-relaxation pseudo-step on ``K_T(u) x = b`` (updates x, vel in place)."""
+        prec = precision or self.precision
+        u = self._check_u(u)
+        for t in (b, minv, x, vel):
+            self._check_u(t)
+        work = self.workspace(prec)
+        check(lib().psx_tet4_dr_step(ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u), ptr(self.mu_e),
+                                     ptr(self.kappa_e), self.mu, self.kappa, PRECISIONS[prec], ptr(b), ptr(minv),
+                                     c1, c2, dt, ptr(x), ptr(vel), ptr(r_out), ptr(work), work.numel(),
+                                     ptr(self.status), _stream_handle()), "psx_tet4_dr_step")
+
     def _check_u(self, u: torch.Tensor) -> torch.Tensor:
         if not isinstance(u, torch.Tensor) or u.device != self.X.device or u.dtype != torch.float64:
             raise ValueError("u must be a float64 tensor on the assembler's device")

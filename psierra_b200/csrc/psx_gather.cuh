@@ -122,11 +122,21 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
     }
 }
 
-// Node item: diagonal block and/or f.
-template <typename KT, int NPE, bool WANT_K, bool WANT_F>
+// Dynamic-relaxation epilogue of a node item (the viscous update of
+// psierra analysis/dynamic_relaxation.py:296-299, 378-382 on the linearised system).
+struct DRArgs {
+  const double* b;
+  const double* minv;
+  double c1, c2, dt;
+  double* x;
+  double* vel;
+};
+
+// Node item: diagonal block and/or f (or, with DR, the fused pseudo-step on f = K x).
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false>
 __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, const KT* __restrict__ krec,
                                             const double* __restrict__ frec, KT* __restrict__ k_out,
-                                            double* __restrict__ f_out) {
+                                            double* __restrict__ f_out, const DRArgs* dr = nullptr) {
   using L = RecLayout<NPE>;
   const int4 info = __ldg(reinterpret_cast<const int4*>(g.node_info) + n);
   const int32_t s0 = __ldg(g.node_ptr + n), s1 = __ldg(g.node_ptr + n + 1);
@@ -177,7 +187,19 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
         for (int m = 0; m < 3; ++m) __stcs(k_out + info.x + (int64_t)info.y * k + m, full[3 * k + m]);
     }
   }
-  if constexpr (WANT_F) {
+  if constexpr (DR) {
+    // every element reading x_i has been evaluated (they are this item's contributions)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int64_t d = 3 * (int64_t)info.z + k;
+      const double r = dr->b[d] - fa[k];
+      const double a = dr->minv[d] * r;
+      const double v = dr->c1 * dr->vel[d] + dr->c2 * a;
+      dr->vel[d] = v;
+      dr->x[d] += dr->dt * v;
+      if (f_out) f_out[d] = r;
+    }
+  } else if constexpr (WANT_F) {
     __stcs(f_out + 3 * (int64_t)info.z + 0, fa[0]);
     __stcs(f_out + 3 * (int64_t)info.z + 1, fa[1]);
     __stcs(f_out + 3 * (int64_t)info.z + 2, fa[2]);

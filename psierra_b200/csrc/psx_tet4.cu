@@ -28,6 +28,7 @@ namespace psx {
 namespace {
 
 constexpr int kThreads = 128;
+constexpr int kModeDR = 16;  // internal: PSX_KV with the fused dynamic-relaxation epilogue
 #ifndef PSX_TET4_MIN_BLOCKS
 #define PSX_TET4_MIN_BLOCKS 2
 #endif
@@ -86,6 +87,7 @@ struct Tet4Args {
   const int32_t* conn;
   const double* X;
   const double* U;
+  const double* Vv;  // vector of the matrix-free product (PSX_KV)
   const double* mu_e;
   const double* kappa_e;
   double mu0, kappa0, lam0;
@@ -100,9 +102,10 @@ template <typename KT, int MODE, bool KGLOBAL = true>
 __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
                                              double* __restrict__ frec) {
   using L = RecLayout<4>;
-  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
+  constexpr bool kKV = (MODE & PSX_KV) != 0;
+  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 && !kKV;
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
-  constexpr bool kWantK = (MODE & PSX_WANT_K) != 0 || kLinear;
+  constexpr bool kWantK = ((MODE & PSX_WANT_K) != 0 || kLinear) && !kKV;
   const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
   double Xn[4][3];
   load_nodes(A.X, cn, Xn);
@@ -146,7 +149,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 #pragma unroll
       for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(fr[2 * i], fr[2 * i + 1]));
     }
-    if constexpr (kWantK) {
+    if constexpr (kWantK || kKV) {
       tc = tangent_coef<KT>(ps, kappa, G.V);
       KT Fi[3][3], Fm[3][3];
 #pragma unroll
@@ -164,6 +167,56 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
           q[b][k] = Fm[k][0] * gk[b][0] + Fm[k][1] * gk[b][1] + Fm[k][2] * gk[b][2];
         }
     }
+  }
+  if constexpr (kKV) {
+    // y_a = sum_b K_ab v_b = alpha p_a + Pv h_a + beta (c q_a) + phi (sum_b (g_a.g_b) v_b)
+    // with alpha = sum_b w_b.v_b, beta = sum_b p_b.v_b, Pv = sum_b p_b v_b^T.
+    // L2 loads: in the fused dynamic-relaxation step the vector is updated in place later
+    // in the same launch (after every element reading a node has been evaluated).
+    double Vn[4][3];
+    {
+      const int ids[4] = {cn.x, cn.y, cn.z, cn.w};
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Vn[b][k] = __ldcg(A.Vv + 3 * (int64_t)ids[b] + k);
+    }
+    KT vk[4][3];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) vk[b][k] = (KT)Vn[b][k];
+    KT alpha = 0, beta = 0, Pv[3][3], Gv[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) Pv[k][m] = Gv[k][m] = (KT)0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        alpha += (tc.A * p[b][k] + tc.c * q[b][k]) * vk[b][k];
+        beta += p[b][k] * vk[b][k];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          Pv[k][m] += p[b][k] * vk[b][m];
+          Gv[k][m] += gk[b][k] * vk[b][m];
+        }
+      }
+    }
+    double yr[12];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        KT t = alpha * p[a][k] + beta * tc.c * q[a][k];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) t += Pv[k][m] * (tc.hb * p[a][m]) + tc.phi * gk[a][m] * Gv[m][k];
+        yr[3 * a + k] = (double)t;
+      }
+    double2* fq = reinterpret_cast<double2*>(frec);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(yr[2 * i], yr[2 * i + 1]));
   }
   if constexpr (kWantK) {
     // K_ab[k][m] = p_a,k w_b,m + p_b,k h_a,m + y_a,k p_b,m + s_ab d_km
@@ -220,10 +273,12 @@ struct StageSmem {
 template <typename KT, int MODE>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
-                       KT* __restrict__ k_out, double* __restrict__ f_out) {
+                       KT* __restrict__ k_out, double* __restrict__ f_out, DRArgs dr) {
   using L = RecLayout<4>;
-  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+  constexpr bool kKV = (MODE & PSX_KV) != 0;
+  constexpr bool kDR = (MODE & kModeDR) != 0;
+  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0 && !kKV;
   const int lane = threadIdx.x & 31;
   int32_t* acnt = Q.counters + 1;
   int32_t* bcnt = Q.counters + 1 + Q.n_granules;
@@ -284,7 +339,7 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
         if (task.x == 1) {
           gather_pair<KT, 4>(g, item, krec, k_out);
         } else {
-          gather_node<KT, 4, kWantK, kWantF>(g, item, krec, frec, k_out, f_out);
+          gather_node<KT, 4, kWantK, kWantF, kDR>(g, item, krec, frec, k_out, f_out, &dr);
         }
       }
       __syncwarp();
@@ -316,8 +371,8 @@ __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double*
 
 template <typename KT, int MODE>
 int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
-             cudaStream_t stream) {
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+             cudaStream_t stream, const DRArgs& dr = DRArgs{}) {
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0 && (MODE & PSX_KV) == 0;
   GatherArgs g;
   g.pair_info = P->pair_info;
   g.pair_ptr = P->pair_ptr;
@@ -346,7 +401,7 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
                            (int)smem) != cudaSuccess)
     return PSX_ERR_CUDA;
   tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
-                                                                      k_out, f_out);
+                                                                      k_out, f_out, dr);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }
@@ -382,7 +437,7 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   int rc = work_layout(plan, precision, work, &W, kMinBlocks);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
-  Tet4Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
+  Tet4Args A{plan->conn, X, u, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define PSX_T4(KT, M) run_tet4<KT, M>(plan, A, W, static_cast<KT*>(k_out), f_out, s)
   if (linear) return precision == PSX_FP64 ? PSX_T4(double, PSX_LINEAR) : PSX_T4(float, PSX_LINEAR);
@@ -391,6 +446,38 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   if (wantK) return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_K) : PSX_T4(float, PSX_WANT_K);
   return PSX_T4(double, PSX_WANT_F);
 #undef PSX_T4
+}
+
+extern "C" int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
+                           const double* kappa_e, double mu, double kappa, int precision, const double* v,
+                           double* y_out, void* work, int64_t work_bytes, void* status, void* stream) {
+  using namespace psx;
+  if (!plan || plan->npe != 4 || !X || !u || !v || !y_out || !status || !work) return PSX_ERR_ARG;
+  WorkLayout W;
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
+  Tet4Args A{plan->conn, X, u, v, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return precision == PSX_FP64 ? run_tet4<double, PSX_KV>(plan, A, W, nullptr, y_out, s)
+                               : run_tet4<float, PSX_KV>(plan, A, W, nullptr, y_out, s);
+}
+
+extern "C" int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
+                                const double* kappa_e, double mu, double kappa, int precision, const double* b,
+                                const double* minv, double c1, double c2, double dt, double* x, double* vel,
+                                double* r_out, void* work, int64_t work_bytes, void* status, void* stream) {
+  using namespace psx;
+  if (!plan || plan->npe != 4 || !X || !u || !b || !minv || !x || !vel || !status || !work) return PSX_ERR_ARG;
+  WorkLayout W;
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
+  Tet4Args A{plan->conn, X, u, x, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
+  DRArgs dr{b, minv, c1, c2, dt, x, vel};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return precision == PSX_FP64 ? run_tet4<double, PSX_KV | kModeDR>(plan, A, W, nullptr, r_out, s, dr)
+                               : run_tet4<float, PSX_KV | kModeDR>(plan, A, W, nullptr, r_out, s, dr);
 }
 
 extern "C" int psx_tet4_element_dets(const int32_t* conn, const double* X, const double* u, int64_t e,
