@@ -222,6 +222,30 @@ int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const double* u,
                      double* x, double* vel, double* r_out, void* work, int64_t work_bytes,
                      void* status, void* stream);
 
+/* ---- Preconditioned CG (device) ---------------------------------------------- */
+
+#define PSX_PRECOND_NONE 0
+#define PSX_PRECOND_JACOBI 1     /* 1/diag where |diag| > 1e-14, else 1 (the reference's) */
+#define PSX_PRECOND_BJACOBI 2    /* inverse 3x3 diagonal block per node (n % 3 == 0) */
+
+/* Workspace bytes of psx_pcg for an n x n system. */
+int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes);
+
+/*
+ * Preconditioned CG on a CSR matrix (replaces solver/sparse_linear_solver.py:37-68,
+ * scipy.sparse.linalg.cg with the Jacobi operator).  indptr (n+1), indices (nnz,
+ * sorted per row), values (nnz; double for PSX_FP64, float for PSX_FP32_MIXED) on the
+ * device; b (n) and x (n, in: initial guess -- zero for the reference's behaviour --,
+ * out: solution) double.  Stops when ||r|| < max(atol, rtol ||b||), as scipy does;
+ * after maxiter updates without that it stops unconverged.  Writes to status:
+ * iters = iterations, flags = 0 converged / 2 max iterations reached / 4 breakdown,
+ * value = final ||r||.  Dot products are reduced in a fixed order (bitwise
+ * reproducible).  Synchronises the stream every 16 iterations to test convergence.
+ */
+int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+            int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+            int precond, void* work, int64_t work_bytes, void* status, void* stream);
+
 /*
  * Reference det (of [1 X], = 6 V) and det F of one element, written to out2
  * (device, 2 doubles).  Used to word the inversion error of a failed call.

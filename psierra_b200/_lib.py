@@ -24,6 +24,10 @@ PSX_KV = 8
 PSX_FP64 = 0
 PSX_FP32_MIXED = 1
 
+PSX_PRECOND_NONE = 0
+PSX_PRECOND_JACOBI = 1
+PSX_PRECOND_BJACOBI = 2
+
 _ERRORS = {
     PSX_ERR_ARG: "invalid argument",
     PSX_ERR_CUDA: "CUDA launch or copy failed",
@@ -51,6 +55,8 @@ SIGNATURES: dict[str, list] = {
     "psx_tet4_dr_step": [_p, _p, _p, _p, _p, _f64, _f64, _i32, _p, _p, _f64, _f64, _f64, _p, _p, _p, _p, _i64,
                          _p, _p],
     "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
+    "psx_pcg_work_bytes": [_i64, _i32, _p],
+    "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
 }
 
 

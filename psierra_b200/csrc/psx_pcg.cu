@@ -1,0 +1,402 @@
+// Preconditioned conjugate gradients on a CSR matrix (sm_100a).
+//
+// Restates the iteration of scipy.sparse.linalg.cg as the reference calls it from
+// ConjugateGradientSolver.solve (psierra solver/sparse_linear_solver.py:37-68):
+//   atol = max(atol, rtol ||b||);  r = b - A x
+//   loop: if ||r|| < atol: converged
+//         z = M^-1 r;  rho = r.z;  p = z (first) | p = z + (rho/rho_prev) p
+//         q = A p;  alpha = rho / p.q;  x += alpha p;  r -= alpha q
+// with the Jacobi preconditioner of the reference (1/diag where |diag| > 1e-14, else 1)
+// or a 3x3 block-Jacobi preconditioner (inverse of each node's diagonal block).
+//
+// Three kernels per iteration: p-update, SpMV (+ p.q), and the fused x/r/z update
+// (+ r.r, r.z).  Every dot product is reduced deterministically: each block reduces its
+// share with a fixed tree and stores a partial; the last block to finish (atomic
+// ticket) sums the partials in index order.  All scalars stay on the device; once
+// converged (or broken down) every kernel returns immediately, so the host only checks
+// the state every few iterations.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "psx_common.cuh"
+
+namespace psx {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kGridMax = 148 * 4;
+constexpr int kRowLanes = 8;  // lanes per CSR row in the SpMV
+
+struct PcgScalars {
+  double rho, rho_prev, pq, alpha, rr, bb, atol2;
+  int32_t converged, breakdown, iters, first;
+  uint32_t ticket[4];
+};
+
+struct PcgWork {
+  double* r;
+  double* z;
+  double* p;
+  double* q;
+  double* minv;   // Jacobi: n; block-Jacobi: 9 per node
+  double* partial;  // 3 * grid
+  PcgScalars* s;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fixed-shape block reduction of up to 3 values; lane 0 of warp 0 gets the sums.
+template <int NV>
+__device__ __forceinline__ void block_sum(double v[NV]) {
+  __shared__ double sm[NV][kBlock / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    const double t = warp_sum(v[i]);
+    if (l == 0) sm[i][w] = t;
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = warp_sum(l < kBlock / 32 ? sm[i][l] : 0.0);
+  }
+  __syncthreads();
+}
+
+// Store this block's partial sums; the last block reduces all partials in index order
+// and returns true (in thread 0) with the totals in `tot`.
+template <int NV>
+__device__ __forceinline__ bool last_block_total(double v[NV], double* partial, uint32_t* ticket, double tot[NV]) {
+  block_sum<NV>(v);
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) partial[i * kGridMax + blockIdx.x] = v[i];
+    __threadfence();
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  for (int bidx = threadIdx.x; bidx < (int)gridDim.x; bidx += kBlock)
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] += __ldcg(partial + i * kGridMax + bidx);
+  block_sum<NV>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) tot[i] = acc[i];
+    *ticket = 0;
+  }
+  return threadIdx.x == 0;
+}
+
+__device__ __forceinline__ bool stopped(const PcgScalars* s) {
+  return *(volatile const int32_t*)&s->converged || *(volatile const int32_t*)&s->breakdown;
+}
+
+// ---- preconditioner setup -----------------------------------------------------------
+__global__ void jacobi_setup(int64_t n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                             const void* __restrict__ vals, int fp32, double* __restrict__ minv, int identity) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t lo = indptr[i], hi = indptr[i + 1] - 1;
+    double d = 0.0;
+    while (lo <= hi) {  // sorted column indices
+      const int32_t mid = (lo + hi) >> 1;
+      const int32_t c = indices[mid];
+      if (c == i) {
+        d = fp32 ? (double)static_cast<const float*>(vals)[mid] : static_cast<const double*>(vals)[mid];
+        break;
+      }
+      if (c < i) lo = mid + 1; else hi = mid - 1;
+    }
+    minv[i] = identity ? 1.0 : (fabs(d) > 1e-14 ? 1.0 / d : 1.0);
+  }
+}
+
+__device__ __forceinline__ double csr_at(const int32_t* indptr, const int32_t* indices, const void* vals, int fp32,
+                                         int64_t row, int64_t col) {
+  int32_t lo = indptr[row], hi = indptr[row + 1] - 1;
+  while (lo <= hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    const int32_t c = indices[mid];
+    if (c == col) return fp32 ? (double)static_cast<const float*>(vals)[mid] : static_cast<const double*>(vals)[mid];
+    if (c < col) lo = mid + 1; else hi = mid - 1;
+  }
+  return 0.0;
+}
+
+__global__ void bjacobi_setup(int64_t nodes, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                              const void* __restrict__ vals, int fp32, double* __restrict__ binv,
+                              PcgScalars* s) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double B[3][3], Bi[3][3];
+    for (int k = 0; k < 3; ++k)
+      for (int m = 0; m < 3; ++m) B[k][m] = csr_at(indptr, indices, vals, fp32, 3 * i + k, 3 * i + m);
+    const double det = inv3(B, Bi);
+    const bool ok = fabs(det) > 1e-300 && isfinite(det);
+    for (int k = 0; k < 3; ++k)
+      for (int m = 0; m < 3; ++m) binv[9 * i + 3 * k + m] = ok ? Bi[k][m] : (k == m ? 1.0 : 0.0);
+  }
+}
+
+// z = M^-1 r for element/node `i`.
+template <bool BLOCK>
+__device__ __forceinline__ void apply_prec(const PcgWork& w, int64_t i, double* __restrict__ z,
+                                           const double* __restrict__ r) {
+  if constexpr (BLOCK) {
+    const double* B = w.minv + 9 * i;
+    const double r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
+    z[3 * i] = B[0] * r0 + B[1] * r1 + B[2] * r2;
+    z[3 * i + 1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
+    z[3 * i + 2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
+  } else {
+    z[i] = w.minv[i] * r[i];
+  }
+}
+
+// ---- SpMV: q = A p (8 lanes per row, fixed-order lane sums) and the p.q partials ------
+template <typename VT>
+__device__ __forceinline__ double spmv_row(int64_t n, int64_t row, int lane8, const int32_t* __restrict__ indptr,
+                                           const int32_t* __restrict__ indices, const VT* __restrict__ vals,
+                                           const double* __restrict__ x) {
+  // rows past the end run the same shuffles with an empty range
+  const int32_t j0 = row < n ? indptr[row] : 0, j1 = row < n ? indptr[row + 1] : 0;
+  double acc = 0.0;
+  for (int32_t j = j0 + lane8; j < j1; j += kRowLanes) acc += (double)vals[j] * __ldcg(x + indices[j]);
+#pragma unroll
+  for (int o = kRowLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+// r = b - A x, z = M^-1 r, and the sums r.r, r.z, b.b (setup of the iteration).
+template <typename VT, bool BLOCK>
+__global__ void __launch_bounds__(kBlock) pcg_init_residual(int64_t n, const int32_t* __restrict__ indptr,
+                                                            const int32_t* __restrict__ indices,
+                                                            const VT* __restrict__ vals, const double* __restrict__ b,
+                                                            const double* __restrict__ x, PcgWork w) {
+  const int lane8 = threadIdx.x & (kRowLanes - 1);
+  const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
+  for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
+    const int64_t row = row0 + threadIdx.x / kRowLanes;
+    const double ax = spmv_row<VT>(n, row, lane8, indptr, indices, vals, x);
+    if (row < n && lane8 == 0) w.r[row] = b[row] - ax;
+  }
+}
+
+template <bool BLOCK>
+__global__ void __launch_bounds__(kBlock) pcg_init_dots(int64_t n, const double* __restrict__ b, PcgWork w,
+                                                        double rtol, double atol) {
+  double v[3] = {0.0, 0.0, 0.0};
+  const int64_t units = BLOCK ? n / 3 : n;
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < units; i += (int64_t)gridDim.x * kBlock) {
+    apply_prec<BLOCK>(w, i, w.z, w.r);
+    const int nd = BLOCK ? 3 : 1;
+    for (int k = 0; k < nd; ++k) {
+      const int64_t d = BLOCK ? 3 * i + k : i;
+      v[0] += w.r[d] * w.r[d];
+      v[1] += w.r[d] * w.z[d];
+      v[2] += b[d] * b[d];
+    }
+  }
+  double tot[3];
+  if (last_block_total<3>(v, w.partial, &w.s->ticket[0], tot)) {
+    PcgScalars* s = w.s;
+    s->rr = tot[0];
+    s->rho = tot[1];
+    s->bb = tot[2];
+    const double a = fmax(atol, rtol * sqrt(tot[2]));
+    s->atol2 = a * a;
+    s->iters = 0;
+    s->first = 1;
+    s->breakdown = 0;
+    // scipy returns x = b (= 0 for x0 = 0 handled by the caller) when ||b|| == 0
+    s->converged = (tot[2] == 0.0 || sqrt(tot[0]) < a) ? 1 : 0;
+  }
+}
+
+// p = z (first iteration) or p = z + beta p
+template <bool BLOCK>
+__global__ void __launch_bounds__(kBlock) pcg_update_p(int64_t n, PcgWork w) {
+  const PcgScalars* s = w.s;
+  if (stopped(s)) return;
+  const bool first = s->first != 0;
+  const double beta = first ? 0.0 : s->rho / s->rho_prev;
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock)
+    w.p[i] = first ? w.z[i] : w.z[i] + beta * w.p[i];
+}
+
+// q = A p and p.q -> alpha = rho / p.q
+template <typename VT>
+__global__ void __launch_bounds__(kBlock) pcg_spmv(int64_t n, const int32_t* __restrict__ indptr,
+                                                   const int32_t* __restrict__ indices, const VT* __restrict__ vals,
+                                                   PcgWork w) {
+  if (stopped(w.s)) return;
+  const int lane8 = threadIdx.x & (kRowLanes - 1);
+  double v[1] = {0.0};
+  const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
+  for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
+    const int64_t row = row0 + threadIdx.x / kRowLanes;
+    const double q = spmv_row<VT>(n, row, lane8, indptr, indices, vals, w.p);
+    if (row < n && lane8 == 0) {
+      w.q[row] = q;
+      v[0] += w.p[row] * q;
+    }
+  }
+  double tot[1];
+  if (last_block_total<1>(v, w.partial, &w.s->ticket[1], tot)) {
+    PcgScalars* s = w.s;
+    s->pq = tot[0];
+    if (!(tot[0] != 0.0) || !isfinite(tot[0])) s->breakdown = 1;
+    s->alpha = s->rho / tot[0];
+  }
+}
+
+// x += alpha p; r -= alpha q; z = M^-1 r; r.r and r.z for the next iteration.
+template <bool BLOCK>
+__global__ void __launch_bounds__(kBlock) pcg_update_xr(int64_t n, double* __restrict__ x, PcgWork w,
+                                                        int32_t maxiter) {
+  PcgScalars* s = w.s;
+  if (stopped(s)) return;
+  const double alpha = s->alpha;
+  double v[2] = {0.0, 0.0};
+  const int64_t units = BLOCK ? n / 3 : n;
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < units; i += (int64_t)gridDim.x * kBlock) {
+    const int nd = BLOCK ? 3 : 1;
+    for (int k = 0; k < nd; ++k) {
+      const int64_t d = BLOCK ? 3 * i + k : i;
+      x[d] += alpha * w.p[d];
+      w.r[d] -= alpha * w.q[d];
+    }
+    apply_prec<BLOCK>(w, i, w.z, w.r);
+    for (int k = 0; k < nd; ++k) {
+      const int64_t d = BLOCK ? 3 * i + k : i;
+      v[0] += w.r[d] * w.r[d];
+      v[1] += w.r[d] * w.z[d];
+    }
+  }
+  double tot[2];
+  if (last_block_total<2>(v, w.partial, &w.s->ticket[2], tot)) {
+    s->rho_prev = s->rho;
+    s->rr = tot[0];
+    s->rho = tot[1];
+    s->first = 0;
+    s->iters += 1;
+    // scipy checks the residual at the top of each of its maxiter iterations, so a
+    // residual reached by the last allowed update still reports non-convergence
+    if (!isfinite(tot[0])) s->breakdown = 1;
+    else if (s->iters >= maxiter) s->breakdown = 2;
+    else if (tot[0] < s->atol2) s->converged = 1;
+  }
+}
+
+__global__ void pcg_report(const PcgScalars* s, Status* st) {
+  st->iters = s->iters;
+  st->flags = s->converged ? 0 : (s->breakdown == 2 ? 2 : 4);
+  st->value = sqrt(s->rr);
+}
+
+size_t up256(size_t b) { return (b + 255) / 256 * 256; }
+
+int layout(int64_t n, int precond, void* work, PcgWork* w, int64_t* bytes) {
+  const size_t vec = up256(sizeof(double) * n);
+  const size_t mv = precond == PSX_PRECOND_BJACOBI ? up256(sizeof(double) * 3 * n) : vec;
+  const size_t part = up256(sizeof(double) * 3 * kGridMax);
+  const size_t sc = up256(sizeof(PcgScalars));
+  *bytes = (int64_t)(4 * vec + mv + part + sc);
+  if (!work) return PSX_OK;
+  if (reinterpret_cast<uintptr_t>(work) & 255) return PSX_ERR_ARG;
+  char* c = static_cast<char*>(work);
+  w->r = reinterpret_cast<double*>(c);
+  w->z = reinterpret_cast<double*>(c + vec);
+  w->p = reinterpret_cast<double*>(c + 2 * vec);
+  w->q = reinterpret_cast<double*>(c + 3 * vec);
+  w->minv = reinterpret_cast<double*>(c + 4 * vec);
+  w->partial = reinterpret_cast<double*>(c + 4 * vec + mv);
+  w->s = reinterpret_cast<PcgScalars*>(c + 4 * vec + mv + part);
+  return PSX_OK;
+}
+
+template <typename VT, bool BLOCK>
+int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* vals, const double* b, double* x,
+            double rtol, double atol, int32_t maxiter, const PcgWork& w, Status* st, cudaStream_t s,
+            int identity) {
+  const int grid_vec = (int)std::min<int64_t>(kGridMax, (n + kBlock - 1) / kBlock);
+  const int grid_row = (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
+  if (cudaMemsetAsync(w.s, 0, sizeof(PcgScalars), s) != cudaSuccess) return PSX_ERR_CUDA;
+  if (BLOCK)
+    bjacobi_setup<<<grid_vec, kBlock, 0, s>>>(n / 3, indptr, indices, vals, sizeof(VT) == 4, w.minv, w.s);
+  else
+    jacobi_setup<<<grid_vec, kBlock, 0, s>>>(n, indptr, indices, vals, sizeof(VT) == 4, w.minv, identity);
+  pcg_init_residual<VT, BLOCK><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, b, x, w);
+  pcg_init_dots<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, b, w, rtol, atol);
+  PSX_CUDA_CHECK_LAUNCH();
+  // iterate in batches; every kernel is a no-op once the state is converged or broken down
+  PcgScalars host;
+  int32_t done = 0;
+  constexpr int kBatchIters = 16;
+  while (done < maxiter) {
+    const int32_t batch = std::min<int32_t>(kBatchIters, maxiter - done);
+    for (int32_t k = 0; k < batch; ++k) {
+      pcg_update_p<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, w);
+      pcg_spmv<VT><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, w);
+      pcg_update_xr<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, x, w, maxiter);
+    }
+    PSX_CUDA_CHECK_LAUNCH();
+    done += batch;
+    if (cudaMemcpyAsync(&host, w.s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return PSX_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PSX_ERR_CUDA;
+    if (host.converged || host.breakdown) break;
+  }
+  pcg_report<<<1, 1, 0, s>>>(w.s, st);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+}  // namespace
+}  // namespace psx
+
+extern "C" int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes) {
+  if (n <= 0 || !bytes || precond < PSX_PRECOND_NONE || precond > PSX_PRECOND_BJACOBI) return PSX_ERR_ARG;
+  if (precond == PSX_PRECOND_BJACOBI && n % 3) return PSX_ERR_ARG;
+  psx::PcgWork w;
+  return psx::layout(n, precond, nullptr, &w, bytes);
+}
+
+extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                       int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+                       int precond, void* work, int64_t work_bytes, void* status, void* stream) {
+  using namespace psx;
+  if (n <= 0 || !indptr || !indices || !values || !b || !x || !work || !status || maxiter < 0) return PSX_ERR_ARG;
+  if (precond < PSX_PRECOND_NONE || precond > PSX_PRECOND_BJACOBI) return PSX_ERR_ARG;
+  if (precond == PSX_PRECOND_BJACOBI && n % 3) return PSX_ERR_ARG;
+  if (value_precision != PSX_FP64 && value_precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  PcgWork w;
+  int64_t need = 0;
+  int rc = layout(n, precond, work, &w, &need);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < need) return PSX_ERR_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Status* st = static_cast<Status*>(status);
+  const bool blk = precond == PSX_PRECOND_BJACOBI;
+  const int id = precond == PSX_PRECOND_NONE;
+  if (value_precision == PSX_FP64) {
+    const double* v = static_cast<const double*>(values);
+    return blk ? run_pcg<double, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id)
+               : run_pcg<double, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id);
+  }
+  const float* v = static_cast<const float*>(values);
+  return blk ? run_pcg<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id)
+             : run_pcg<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id);
+}
