@@ -46,6 +46,7 @@ extern "C" {
 #define PSX_WANT_K 2            /* tangent stiffness K_T(u) values in the CSR pattern */
 #define PSX_LINEAR 4            /* small-strain stiffness from (lambda, mu); ignores u */
 #define PSX_KV 8                /* matrix-free product y = K_T(u) v (psx_tet4_kv) */
+#define PSX_MASS 32             /* consistent mass matrix; `lam` carries the density */
 
 /* Precision of the element tangent (`precision`) */
 #define PSX_FP64 0              /* everything in FP64, K values stored as double */
@@ -182,7 +183,8 @@ int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t* ring_elems, i
  * domain/solid.py:172-207, 230-325 and the COO->CSR / np.add.at scatter).
  *   X, u (device, N x 3 double; u ignored for PSX_LINEAR)
  *   mu_e, kappa_e (device, E doubles) per-element moduli, or NULL to use mu, kappa
- *   lam: Lame lambda for PSX_LINEAR (with mu)
+ *   lam: Lame lambda for PSX_LINEAR (with mu); the mass density for PSX_MASS
+ *        (element/tet4_base.py:138-151: rho V / 20 (1 + delta_ab) I per block)
  *   f_out (device, 3N doubles) when mode has PSX_WANT_F
  *   k_out (device, nnz values in psx_csr_pattern order: double for PSX_FP64, float
  *          for PSX_FP32_MIXED) when mode has PSX_WANT_K or PSX_LINEAR

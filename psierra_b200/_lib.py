@@ -20,6 +20,7 @@ PSX_WANT_F = 1
 PSX_WANT_K = 2
 PSX_LINEAR = 4
 PSX_KV = 8
+PSX_MASS = 32
 
 PSX_FP64 = 0
 PSX_FP32_MIXED = 1

@@ -108,23 +108,24 @@ class GPUAssembler:
     # ------------------------------------------------------------------ kernels
     def assemble(self, u: torch.Tensor | None, want_f: bool = True, want_k: bool = True,
                  precision: str | None = None, f_out: torch.Tensor | None = None,
-                 k_out: torch.Tensor | None = None, check_status: bool = True, linear: bool = False):
+                 k_out: torch.Tensor | None = None, check_status: bool = True, linear: bool = False,
+                 mass: bool = False):
         """One sweep over all elements.  Returns ``(f, k)``; either may be None.
 
         ``u`` is the ``(N, 3)`` (or ``(3N,)``) float64 displacement on the device.
         ``k`` holds the CSR values in ``pattern.indptr``/``indices`` order (float64,
         or float32 for ``precision="fp32-mixed"``).  With ``linear=True`` the
-        small-strain stiffness of the reference configuration is assembled instead
-        (``u`` is ignored).
+        small-strain stiffness of the reference configuration is assembled instead, and
+        with ``mass=True`` the consistent mass matrix (``u`` is ignored for both).
         """
         prec = precision or self.precision
         if prec not in PRECISIONS:
             raise ValueError(f"unknown precision {prec!r}")
         if self.npe != 4:
             raise NotImplementedError("Tet10 assembly is provided by psierra_b200.tet10")
-        if linear:
-            mode = _lib.PSX_LINEAR
-            want_f, want_k = False, True
+        if linear or mass:
+            mode = _lib.PSX_MASS if mass else _lib.PSX_LINEAR
+            want_f, want_k, linear = False, True, True
         else:
             mode = (_lib.PSX_WANT_F if want_f else 0) | (_lib.PSX_WANT_K if want_k else 0)
             if mode == 0:
@@ -140,7 +141,8 @@ class GPUAssembler:
         work = self.workspace(prec)
         rc = lib().psx_tet4_assemble(
             ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u) if not linear else None,
-            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.lam, mode, PRECISIONS[prec],
+            ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.rho if mass else self.lam, mode,
+            PRECISIONS[prec],
             ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(work), work.numel(),
             ptr(self.status), _stream_handle())
         check(rc, "psx_tet4_assemble")

@@ -105,6 +105,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   constexpr bool kKV = (MODE & PSX_KV) != 0;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 && !kKV;
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
+  constexpr bool kMass = (MODE & PSX_MASS) != 0;
   constexpr bool kWantK = ((MODE & PSX_WANT_K) != 0 || kLinear) && !kKV;
   const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
   double Xn[4][3];
@@ -112,6 +113,17 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   Tet4Geom G;
   tet4_geometry(Xn, G);
   if (!(G.detD > 0.0)) flag_bad_element(A.st, e, true);
+  if constexpr (kMass) {
+    // tet4_base.py:138-151 with the volume of the mesh (|det| / 6, domain/solid.py:209-228)
+    const KT mm = (KT)(A.lam0 * fabs(G.V) / 20.0);
+    const KT off[9] = {mm, 0, 0, 0, mm, 0, 0, 0, mm};
+    const KT d[6] = {(KT)2 * mm, 0, 0, (KT)2 * mm, 0, (KT)2 * mm};
+#pragma unroll
+    for (int slot = 0; slot < 6; ++slot) store_pair_block<KT, KGLOBAL>(krec + L::pair_off(slot), off, false);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) store_diag_block<KT, KGLOBAL>(krec + L::diag_off(a), d);
+    return;
+  }
   KT p[4][3], q[4][3];
   TangentCoef<KT> tc;
   KT gk[4][3];
@@ -278,7 +290,7 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
   constexpr bool kKV = (MODE & PSX_KV) != 0;
   constexpr bool kDR = (MODE & kModeDR) != 0;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0 && !kKV;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && !kKV;
   const int lane = threadIdx.x & 31;
   int32_t* acnt = Q.counters + 1;
   int32_t* bcnt = Q.counters + 1 + Q.n_granules;
@@ -372,7 +384,7 @@ __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double*
 template <typename KT, int MODE>
 int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
              cudaStream_t stream, const DRArgs& dr = DRArgs{}) {
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0 && (MODE & PSX_KV) == 0;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && (MODE & PSX_KV) == 0;
   GatherArgs g;
   g.pair_info = P->pair_info;
   g.pair_ptr = P->pair_ptr;
@@ -428,7 +440,8 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   using namespace psx;
   if (!plan || plan->npe != 4 || !X || !status || !work) return PSX_ERR_ARG;
   const bool wantF = (mode & PSX_WANT_F) != 0, wantK = (mode & PSX_WANT_K) != 0,
-             linear = (mode & PSX_LINEAR) != 0;
+             mass = (mode & PSX_MASS) != 0, linear = (mode & PSX_LINEAR) != 0 || mass;
+  if ((mode & PSX_LINEAR) && mass) return PSX_ERR_ARG;
   if (linear && (wantF || wantK || !k_out)) return PSX_ERR_ARG;
   if (!linear && (!(wantF || wantK) || !u)) return PSX_ERR_ARG;
   if (wantF && !f_out) return PSX_ERR_ARG;
@@ -440,6 +453,7 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   Tet4Args A{plan->conn, X, u, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define PSX_T4(KT, M) run_tet4<KT, M>(plan, A, W, static_cast<KT*>(k_out), f_out, s)
+  if (mass) return precision == PSX_FP64 ? PSX_T4(double, PSX_MASS) : PSX_T4(float, PSX_MASS);
   if (linear) return precision == PSX_FP64 ? PSX_T4(double, PSX_LINEAR) : PSX_T4(float, PSX_LINEAR);
   if (wantF && wantK)
     return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_F | PSX_WANT_K) : PSX_T4(float, PSX_WANT_F | PSX_WANT_K);

@@ -148,6 +148,12 @@ class _GPUElementBase:
         _, k = asm.assemble(None, linear=True)
         return self._csr(k)
 
+    def assemble_mass_matrix(self, mesh) -> spsp.csr_matrix:
+        """Consistent mass matrix (psierra ``domain/solid.py:209-228`` with ``compute_mass_matrix``)."""
+        asm = self._setup(mesh)
+        _, k = asm.assemble(None, mass=True)
+        return self._csr(k)
+
     def assemble_force_and_tangent(self, mesh, displacement) -> tuple[np.ndarray, spsp.csr_matrix]:
         """Both outputs from one fused element sweep."""
         asm = self._setup(mesh)

@@ -1,0 +1,84 @@
+"""Host logic of the drivers with an analytic fake domain (no GPU), in the manner of the
+reference's SpringDomain tests (psierra tests/test_analysis_solver_foundation.py)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import scipy.sparse as spsp
+
+from psierra_b200.analysis import ContactAwareLineSearch, NonlinearStaticAnalysis, is_element_inversion_error
+from psierra_b200.domain import DirichletManager
+
+
+class SpringDomain:
+    """Two hardening springs in series: f_int = k (u + u^3) per spring (exact tangent)."""
+
+    def __init__(self, k=10.0):
+        self.k = k
+        self.u = np.zeros(3)
+        self.v = np.zeros(3)
+        self.a = np.zeros(3)
+        self.n_dofs = 3
+
+    def update_state(self, u=None, v=None, a=None):
+        if u is not None:
+            self.u[:] = u
+
+    def commit_state(self):
+        pass
+
+    def _e(self):
+        return np.diff(self.u)
+
+    def assemble_internal_forces(self):
+        e = self._e()
+        s = self.k * (e + e ** 3)
+        f = np.zeros(3)
+        f[:2] -= s
+        f[1:] += s
+        return f
+
+    def assemble_tangent_stiffness_matrix(self):
+        e = self._e()
+        kk = self.k * (1 + 3 * e ** 2)
+        K = np.zeros((3, 3))
+        for i, c in enumerate(kk):
+            K[i:i + 2, i:i + 2] += c * np.array([[1, -1], [-1, 1]])
+        return spsp.csr_matrix(K)
+
+
+def test_newton_converges_quadratically_on_springs():
+    dom = SpringDomain()
+    dm = DirichletManager(3)
+    from psierra_b200.domain import DirichletConstraint
+
+    dm.add_constraint(DirichletConstraint([0], components=(0,), value=0.0, dofs_per_node=1))
+    f = np.array([0.0, 0.0, 25.0])
+    r = NonlinearStaticAnalysis(dom).solve(dm, f_ext=f, n_steps=2, nr_iterations=20, nr_tol=1e-12)
+    assert r.converged and r.steps_completed == 2
+    e = np.diff(r.displacement)
+    assert np.allclose(10.0 * (e + e ** 3), 25.0, rtol=1e-10)
+    assert np.allclose(r.reactions[1:], 0.0, atol=1e-9)
+
+
+def test_line_search_rules():
+    ls = ContactAwareLineSearch()
+    # strict decrease at the full step
+    assert ls.search(lambda a: 0.5, 1.0, 1e-9).alpha == 1.0
+    # inversion at the full step, decrease at half
+    def f(a):
+        if a > 0.6:
+            raise ValueError("Element inversion detected: det(F) = -1.0000e-01 <= 0.")
+        return 0.9
+    r = ls.search(f, 1.0, 1e-9)
+    assert r.success and r.alpha == 0.5 and r.element_inversion_encountered
+    # no admissible trial at all
+    def g(a):
+        raise ValueError("Element inversion detected: det(F) = -1.0000e-01 <= 0.")
+    r = ls.search(g, 1.0, 1e-9)
+    assert not r.success and "inversion" in r.rejection_reason
+    # unrelated errors propagate
+    with pytest.raises(KeyError):
+        ls.search(lambda a: (_ for _ in ()).throw(KeyError("x")), 1.0, 1e-9)
+    assert is_element_inversion_error(ValueError("Element inversion detected: det(F) = 0 <= 0."))
+    assert not is_element_inversion_error(ValueError("something else"))
