@@ -249,6 +249,25 @@ int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void
             int precond, void* work, int64_t work_bytes, void* status, void* stream);
 
 /*
+ * psx_pcg without a workspace argument: no counterpart in the reference.  For callers
+ * that cannot allocate device memory when they solve (their device memory belongs to
+ * their own pool allocator, or their run reserves all memory up front), the solve runs
+ * on a fixed 32 MiB scratch array that is part of this library and is reserved on every
+ * GPU that loads it until the process exits (psx_pcg_static_max_bytes() returns the
+ * size).  It allocates nothing.  Systems whose psx_pcg_work_bytes exceeds the scratch
+ * are rejected with PSX_ERR_LIMIT: about n <= 838,000 unknowns with the Jacobi
+ * preconditioner and n <= 599,000 with block-Jacobi.  The first call on a device looks up
+ * the scratch address on that device; make that first call before any stream capture.
+ * Every call on a device shares the one array, so calls that overlap on the GPU (other
+ * streams, other host threads) race; the scalars the solve needs at zero are cleared at
+ * the start of every call.  Arguments and results are those of psx_pcg.
+ */
+size_t psx_pcg_static_max_bytes(void);
+int psx_pcg_static(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                   int value_precision, const double* b, double* x, double rtol, double atol,
+                   int32_t maxiter, int precond, void* status, void* stream);
+
+/*
  * Reference det (of [1 X], = 6 V) and det F of one element, written to out2
  * (device, 2 doubles).  Used to word the inversion error of a failed call.
  */

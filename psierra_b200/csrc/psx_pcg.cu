@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "psx_common.cuh"
 
@@ -399,4 +400,60 @@ extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices,
   const float* v = static_cast<const float*>(values);
   return blk ? run_pcg<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id)
              : run_pcg<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id);
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant: psx_pcg_static.
+//
+// Some callers cannot hand this library a workspace.  A host code that owns all device
+// memory through its own pool (a solver framework's arena, or PyTorch's caching
+// allocator) cannot let a library call cudaMalloc behind its back: the allocation
+// escapes the pool's accounting and implicitly synchronises the device.  A time-stepping
+// loop that reserves its device memory up front may also forbid allocation mid-run.  For
+// them the CG solve can run on scratch that is part of this library's image: a fixed
+// array in device global memory, reserved on every GPU that loads the library until the
+// process exits.
+namespace {
+
+constexpr size_t kStaticPcgBytes = size_t(32) << 20;  // 32 MiB of scratch per GPU
+__device__ __align__(256) unsigned char g_pcg_scratch[kStaticPcgBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_pcg_scratch_addr[kMaxDevices] = {};
+std::mutex g_pcg_scratch_mu;
+
+// Device address of the scratch array on the current device, looked up once per device
+// with that device current (the host-side symbol is only a stand-in, not an address).
+int static_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PSX_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return PSX_ERR_LIMIT;
+  std::lock_guard<std::mutex> lock(g_pcg_scratch_mu);
+  if (!g_pcg_scratch_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_pcg_scratch) != cudaSuccess || !p) return PSX_ERR_CUDA;
+    g_pcg_scratch_addr[dev] = p;
+  }
+  *out = g_pcg_scratch_addr[dev];
+  return PSX_OK;
+}
+
+}  // namespace
+
+extern "C" size_t psx_pcg_static_max_bytes(void) { return kStaticPcgBytes; }
+
+extern "C" int psx_pcg_static(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                              int value_precision, const double* b, double* x, double rtol, double atol,
+                              int32_t maxiter, int precond, void* status, void* stream) {
+  int64_t need = 0;
+  int rc = psx_pcg_work_bytes(n, precond, &need);
+  if (rc != PSX_OK) return rc;
+  if (need > (int64_t)kStaticPcgBytes) return PSX_ERR_LIMIT;  // system too large for the fixed scratch
+  void* scratch = nullptr;
+  rc = static_scratch(&scratch);
+  if (rc != PSX_OK) return rc;
+  // psx_pcg clears the solver scalars and counters at the start of every call and
+  // writes every vector before reading it, so the previous call's contents do not leak.
+  return psx_pcg(n, indptr, indices, values, value_precision, b, x, rtol, atol, maxiter, precond, scratch,
+                 (int64_t)kStaticPcgBytes, status, stream);
 }
