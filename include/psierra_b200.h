@@ -134,8 +134,10 @@ typedef struct psx_plan {
   const int32_t* node_src;  /* device, e * 16 + local node index */
   const int32_t* pair_gptr; /* host, n_granules + 1: pair items ready in each granule */
   const int32_t* node_gptr; /* host, n_granules + 1 */
-  int32_t tile;             /* items per task (psx_task_fill) */
+  int32_t tile;             /* elements per element task (psx_task_fill) */
   int32_t lag;              /* granules between an element tile and the gathers it completes */
+  int32_t tile_items;       /* items per gather task */
+  int32_t pad_;
   int64_t n_tasks_k;        /* task queue with pair tiles (any request involving K) */
   int64_t n_tasks_f;        /* task queue without pair tiles (f only) */
   const int32_t* tasks_k;   /* device, 4 per task: kind, granule, begin, end */
@@ -163,12 +165,14 @@ int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int3
  * Task queue of the persistent assembly kernel (host): for each granule g, the
  * element tiles of g followed by the gather tiles made ready by granule g-1-lag
  * (pairs when with_pairs, then nodes).  Each task is 4 int32 {kind, granule, begin, end};
- * b_tiles_per_granule (n_granules) counts the gather tiles of each granule.  `tile` must
- * divide the plan granule.  Uses only the host fields of `plan`.
+ * b_tiles_per_granule (n_granules) counts the gather tiles of each granule.  Element
+ * tasks hold `tile` elements (dividing the plan granule), gather tasks `tile_items`
+ * items.  Uses only the host fields of `plan`.
  */
-int psx_task_count(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t lag, int64_t* n_tasks);
-int psx_task_fill(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t lag, int32_t* tasks,
-                  int32_t* b_tiles_per_granule);
+int psx_task_count(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t tile_items, int32_t lag,
+                   int64_t* n_tasks);
+int psx_task_fill(const psx_plan_t* plan, int with_pairs, int32_t tile, int32_t tile_items, int32_t lag,
+                  int32_t* tasks, int32_t* b_tiles_per_granule);
 
 /*
  * Workspace bytes of one assembly call on the current device: task counters and a
@@ -198,6 +202,24 @@ int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u,
                       const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,
                       int mode, int precision, double* f_out, void* k_out, void* work,
                       int64_t work_bytes, void* status, void* stream);
+
+/* ---- Tet10 element kernels (device) ---------------------------------------- */
+
+/*
+ * Tet10 Total-Lagrangian NeoHookean assembly, 4-point rule (replaces the element loops of
+ * domain/solid.py:172-207, 230-325 around element/tet10_total_lagrangian.py:63-136 and
+ * element/tet10_base.py:310-342).  Same arguments and outputs as psx_tet4_assemble;
+ * modes PSX_WANT_F, PSX_WANT_K, PSX_LINEAR.  The plan must be built with npe = 10 and an
+ * element task tile of 8.
+ */
+int psx_tet10_assemble(const psx_plan_t* plan, const double* X, const double* u,
+                       const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,
+                       int mode, int precision, double* f_out, void* k_out, void* work,
+                       int64_t work_bytes, void* status, void* stream);
+
+/* det J and det F at the 4 quadrature points of element e: out8 (device, 8 doubles). */
+int psx_tet10_element_dets(const int32_t* conn, const double* X, const double* u, int64_t e,
+                           double* out8, void* stream);
 
 /*
  * Matrix-free tangent product y = K_T(u) v (no matrix is formed): each element

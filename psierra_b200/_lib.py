@@ -48,14 +48,16 @@ SIGNATURES: dict[str, list] = {
     "psx_block_lists": [_p, _i64, _i32, _i64, _p, _p, _p, _p],
     "psx_plan_count": [_p, _i64, _i32, _i64, _p, _p, _p],
     "psx_plan_fill": [_p, _i64, _i32, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _p, _p, _p],
-    "psx_task_count": [_p, _i32, _i32, _i32, _p],
-    "psx_task_fill": [_p, _i32, _i32, _i32, _p, _p],
+    "psx_task_count": [_p, _i32, _i32, _i32, _i32, _p],
+    "psx_task_fill": [_p, _i32, _i32, _i32, _i32, _p, _p],
     "psx_work_bytes": [_p, _i32, _p, _p],
     "psx_tet4_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _p, _p, _p, _i64, _p, _p],
     "psx_tet4_kv": [_p, _p, _p, _p, _p, _f64, _f64, _i32, _p, _p, _p, _i64, _p, _p],
     "psx_tet4_dr_step": [_p, _p, _p, _p, _p, _f64, _f64, _i32, _p, _p, _f64, _f64, _f64, _p, _p, _p, _p, _i64,
                          _p, _p],
     "psx_tet4_element_dets": [_p, _p, _p, _i64, _p, _p],
+    "psx_tet10_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _p, _p, _p, _i64, _p, _p],
+    "psx_tet10_element_dets": [_p, _p, _p, _i64, _p, _p],
     "psx_pcg_work_bytes": [_i64, _i32, _p],
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
 }
@@ -84,6 +86,8 @@ class PlanStruct(ctypes.Structure):
         ("node_gptr", ctypes.c_void_p),
         ("tile", ctypes.c_int32),
         ("lag", ctypes.c_int32),
+        ("tile_items", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
         ("n_tasks_k", ctypes.c_int64),
         ("n_tasks_f", ctypes.c_int64),
         ("tasks_k", ctypes.c_void_p),

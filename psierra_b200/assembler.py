@@ -53,7 +53,7 @@ class GPUAssembler:
         self.X = torch.from_numpy(nodes).to(self.device)
         nbytes = int(lib().psx_status_bytes())
         self.status = torch.zeros((nbytes + 3) // 4, dtype=torch.int32, device=self.device)
-        self._dets = torch.zeros(2, dtype=torch.float64, device=self.device)
+        self._dets = torch.zeros(8, dtype=torch.float64, device=self.device)
         self._work: dict = {}
         self.set_material(material)
 
@@ -121,8 +121,8 @@ class GPUAssembler:
         prec = precision or self.precision
         if prec not in PRECISIONS:
             raise ValueError(f"unknown precision {prec!r}")
-        if self.npe != 4:
-            raise NotImplementedError("Tet10 assembly is provided by psierra_b200.tet10")
+        if self.npe == 10 and mass:
+            raise NotImplementedError("the Tet10 consistent mass is assembled on the host by the reference domain")
         if linear or mass:
             mode = _lib.PSX_MASS if mass else _lib.PSX_LINEAR
             want_f, want_k, linear = False, True, True
@@ -139,13 +139,14 @@ class GPUAssembler:
             raise ValueError(f"k_out must be {self.k_dtype(prec)} for precision {prec}")
         self.status.zero_()
         work = self.workspace(prec)
-        rc = lib().psx_tet4_assemble(
+        entry = lib().psx_tet4_assemble if self.npe == 4 else lib().psx_tet10_assemble
+        rc = entry(
             ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u) if not linear else None,
             ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa, self.rho if mass else self.lam, mode,
             PRECISIONS[prec],
             ptr(f_out) if want_f else None, ptr(k_out) if want_k else None, ptr(work), work.numel(),
             ptr(self.status), _stream_handle())
-        check(rc, "psx_tet4_assemble")
+        check(rc, "psx_tet4_assemble" if self.npe == 4 else "psx_tet10_assemble")
         if check_status:
             self.raise_on_bad_elements(u)
         return (f_out if want_f else None), (k_out if want_k else None)
@@ -205,9 +206,20 @@ class GPUAssembler:
             raise RuntimeError("psierra_b200: a bounded wait in the assembly kernel gave up; results are invalid")
         if n_inv == 0 and n_vol == 0:
             return
+        if self.npe == 10:
+            # tet10_total_lagrangian.py:104-113: quadrature points in order, det J then det F
+            check(lib().psx_tet10_element_dets(ptr(self.dev["conn"]), ptr(self.X), ptr(u), first,
+                                               ptr(self._dets), _stream_handle()), "psx_tet10_element_dets")
+            d = self._dets.cpu().numpy()
+            for q in range(4):
+                if not d[2 * q] > 0.0:
+                    raise ValueError(f"Negative or zero Jacobian determinant: det(J) = {d[2 * q]:.4e}.")
+                if not d[2 * q + 1] > 0.0:
+                    raise ValueError(f"Element inversion detected: det(F) = {d[2 * q + 1]:.4e} <= 0.")
+            raise ValueError("Element inversion detected: det(F) <= 0.")
         check(lib().psx_tet4_element_dets(ptr(self.dev["conn"]), ptr(self.X), ptr(u), first,
                                           ptr(self._dets), _stream_handle()), "psx_tet4_element_dets")
-        detA, J = (float(v) for v in self._dets.cpu().numpy())
+        detA, J = (float(v) for v in self._dets.cpu().numpy()[:2])
         if not detA > 0.0:
             raise ValueError(
                 f"Negative or zero element volume detected (det(A) = {detA}). Check element vertex ordering.")

@@ -278,6 +278,74 @@ __device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first,
 }
 
 
+// ---- persistent queue loop -----------------------------------------------------------
+// Each warp claims tasks in queue order (the claim of the next task is issued before the
+// current one is worked on).  Element tiles wait until the gather tiles still reading
+// the ring slots they overwrite are done, run `element_tile(task)` and publish their
+// granule; gather tiles wait for the element granules they read and sum them.  Every
+// wait is on a task earlier in the queue (psx_task_fill), so the queue always drains.
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR, typename ElementTile>
+__device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs& Q, Status* st,
+                                            const KT* __restrict__ krec, const double* __restrict__ frec,
+                                            KT* __restrict__ k_out, double* __restrict__ f_out, const DRArgs& dr,
+                                            ElementTile&& element_tile) {
+  const int lane = threadIdx.x & 31;
+  int32_t* acnt = Q.counters + 1;
+  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
+  const int64_t gsize = (int64_t)1 << Q.granule_log2;
+  auto atiles = [&](int32_t r) -> int32_t {
+    const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
+    return (int32_t)((n + Q.tile - 1) / Q.tile);
+  };
+  auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  int32_t next = 0;
+  if (lane == 0) next = atomicAdd(Q.counters, 1);
+  while (true) {
+    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
+    if (t >= Q.n_tasks) break;
+    if (lane == 0) next = atomicAdd(Q.counters, 1);
+    const int4 task = __ldg(Q.tasks + t);
+    const int32_t gr = task.y;
+    if (task.x == 0) {
+      const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
+      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st);
+      __syncwarp();
+      element_tile(task);
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        atomicAdd(acnt + gr, 1);
+      }
+    } else {
+      const int32_t first = max(0, gr - Q.span_g - 1);
+      wait_counters(acnt, first, gr - first + 1, atiles, st);
+      __syncwarp();
+      for (int32_t item = task.z + lane; item < task.w; item += 32) {
+        if (task.x == 1) {
+          if constexpr (WANT_K) gather_pair<KT, NPE>(g, item, krec, k_out);
+        } else {
+          gather_node<KT, NPE, WANT_K, WANT_F, DR>(g, item, krec, frec, k_out, f_out, &dr);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) atomicAdd(bcnt + gr, 1);
+    }
+  }
+}
+
+inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
+  GatherArgs g;
+  g.pair_info = P->pair_info;
+  g.pair_ptr = P->pair_ptr;
+  g.pair_src = P->pair_src;
+  g.node_info = P->node_info;
+  g.node_ptr = P->node_ptr;
+  g.node_src = P->node_src;
+  g.p0 = g.p1 = g.n0 = g.n1 = 0;
+  g.ring_mask = ring_elems - 1;
+  return g;
+}
+
 // ---- workspace layout (host side) ---------------------------------------------------
 struct WorkLayout {
   int32_t* counters;

@@ -328,8 +328,10 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
 // tiles from being claimed while the element tiles they read are still running.  Task = int4
 // {kind, granule, begin, end}: kind 0 = element tile [begin, end), 1 = pair items,
 // 2 = node items.  `with_pairs` = 0 builds the f-only queue (no pair tiles).
-extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t lag, int64_t* n_tasks) {
-  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || lag < 0 || !n_tasks)
+extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t tile_items, int32_t lag,
+                              int64_t* n_tasks) {
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || tile_items <= 0 || P->granule % tile || lag < 0 ||
+      !n_tasks)
     return PSX_ERR_ARG;
   int64_t n = 0;
   const int64_t G = P->n_granules;
@@ -340,19 +342,19 @@ extern "C" int psx_task_count(const psx_plan_t* P, int with_pairs, int32_t tile,
     }
     if (g >= 1 + lag && g - 1 - lag < G) {
       const int64_t r = g - 1 - lag;
-      if (with_pairs) n += (P->pair_gptr[r + 1] - P->pair_gptr[r] + tile - 1) / tile;
+      if (with_pairs) n += (P->pair_gptr[r + 1] - P->pair_gptr[r] + tile_items - 1) / tile_items;
       const int64_t n0 = r == 0 ? 0 : P->node_gptr[r];
-      n += (P->node_gptr[r + 1] - n0 + tile - 1) / tile;
+      n += (P->node_gptr[r + 1] - n0 + tile_items - 1) / tile_items;
     }
   }
   *n_tasks = n;
   return PSX_OK;
 }
 
-extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t lag, int32_t* tasks,
-                             int32_t* b_tiles_per_granule) {
-  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || P->granule % tile || lag < 0 || !tasks ||
-      !b_tiles_per_granule)
+extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, int32_t tile_items, int32_t lag,
+                             int32_t* tasks, int32_t* b_tiles_per_granule) {
+  if (!P || !P->pair_gptr || !P->node_gptr || tile <= 0 || tile_items <= 0 || P->granule % tile || lag < 0 ||
+      !tasks || !b_tiles_per_granule)
     return PSX_ERR_ARG;
   const int64_t G = P->n_granules;
   int64_t k = 0;
@@ -372,11 +374,11 @@ extern "C" int psx_task_fill(const psx_plan_t* P, int with_pairs, int32_t tile, 
       const int64_t r = g - 1 - lag;
       int32_t nb = 0;
       if (with_pairs)
-        for (int64_t b = P->pair_gptr[r]; b < P->pair_gptr[r + 1]; b += tile, ++nb)
-          push(1, r, b, std::min<int64_t>(P->pair_gptr[r + 1], b + tile));
+        for (int64_t b = P->pair_gptr[r]; b < P->pair_gptr[r + 1]; b += tile_items, ++nb)
+          push(1, r, b, std::min<int64_t>(P->pair_gptr[r + 1], b + tile_items));
       const int64_t n0 = r == 0 ? 0 : P->node_gptr[r];
-      for (int64_t b = n0; b < P->node_gptr[r + 1]; b += tile, ++nb)
-        push(2, r, b, std::min<int64_t>(P->node_gptr[r + 1], b + tile));
+      for (int64_t b = n0; b < P->node_gptr[r + 1]; b += tile_items, ++nb)
+        push(2, r, b, std::min<int64_t>(P->node_gptr[r + 1], b + tile_items));
       b_tiles_per_granule[r] = nb;
     }
   }

@@ -292,72 +292,33 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && !kKV;
   const int lane = threadIdx.x & 31;
-  int32_t* acnt = Q.counters + 1;
-  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
-  const int64_t gsize = (int64_t)1 << Q.granule_log2;
-  auto atiles = [&](int32_t r) -> int32_t {
-    const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
-    return (int32_t)((n + Q.tile - 1) / Q.tile);
-  };
-  auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
   constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
   extern __shared__ __align__(16) float s_stage[];  // kThreads/32 warps x kWarpFloats (FP32 K only)
   float* my_stage = s_stage + (threadIdx.x >> 5) * StageSmem<KT>::kWarpFloats;
-  // the claim of the next task is issued before the current one is worked on
-  int32_t next = 0;
-  if (lane == 0) next = atomicAdd(Q.counters, 1);
-  while (true) {
-    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
-    if (t >= Q.n_tasks) break;
-    if (lane == 0) next = atomicAdd(Q.counters, 1);
-    const int4 task = __ldg(Q.tasks + t);
-    const int32_t gr = task.y;
-    if (task.x == 0) {
-      const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, A.st);
+  auto element_tile = [&](const int4& task) {
+    if constexpr (kStage) {
+      // tiles are 32 consecutive elements inside one granule: their ring slots are contiguous
+      const int64_t e = task.z + (int64_t)lane;
+      const int64_t slot0 = (int64_t)task.z & g.ring_mask;
+      if (e < task.w)
+        tet4_element<KT, MODE, false>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
+                                      frec + (e & g.ring_mask) * L::kF);
       __syncwarp();
-      if constexpr (kStage) {
-        // tiles are 32 consecutive elements inside one granule: their ring slots are contiguous
-        const int64_t e = task.z + (int64_t)lane;
-        const int64_t slot0 = (int64_t)task.z & g.ring_mask;
-        if (e < task.w)
-          tet4_element<KT, MODE, false>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
-                                        frec + (e & g.ring_mask) * L::kF);
-        __syncwarp();
-        const int n = task.w - task.z;
-        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(krec) + slot0 * L::kK);
-        constexpr int kChunks = L::kK / 4;  // float4 per record
-        for (int c = lane; c < n * kChunks; c += 32) {
-          const int el = c / kChunks, q = c - el * kChunks;
-          __stcg(dst + c, *reinterpret_cast<const float4*>(my_stage + el * kStageStride + 4 * q));
-        }
-        __syncwarp();
-      } else {
-        for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
-          const int64_t slot = e & g.ring_mask;
-          tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
-        }
-        __syncwarp();
-      }
-      if (lane == 0) {
-        __threadfence();
-        atomicAdd(acnt + gr, 1);
+      const int n = task.w - task.z;
+      float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(krec) + slot0 * L::kK);
+      constexpr int kChunks = L::kK / 4;  // float4 per record
+      for (int c = lane; c < n * kChunks; c += 32) {
+        const int el = c / kChunks, q = c - el * kChunks;
+        __stcg(dst + c, *reinterpret_cast<const float4*>(my_stage + el * kStageStride + 4 * q));
       }
     } else {
-      const int32_t first = max(0, gr - Q.span_g - 1);
-      wait_counters(acnt, first, gr - first + 1, atiles, A.st);
-      __syncwarp();
-      for (int32_t item = task.z + lane; item < task.w; item += 32) {
-        if (task.x == 1) {
-          gather_pair<KT, 4>(g, item, krec, k_out);
-        } else {
-          gather_node<KT, 4, kWantK, kWantF, kDR>(g, item, krec, frec, k_out, f_out, &dr);
-        }
+      for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
+        const int64_t slot = e & g.ring_mask;
+        tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
       }
-      __syncwarp();
-      if (lane == 0) atomicAdd(bcnt + gr, 1);
     }
-  }
+  };
+  drain_queue<KT, 4, kWantK, kWantF, kDR>(g, Q, A.st, krec, frec, k_out, f_out, dr, element_tile);
 }
 
 __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
@@ -385,15 +346,7 @@ template <typename KT, int MODE>
 int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
              cudaStream_t stream, const DRArgs& dr = DRArgs{}) {
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && (MODE & PSX_KV) == 0;
-  GatherArgs g;
-  g.pair_info = P->pair_info;
-  g.pair_ptr = P->pair_ptr;
-  g.pair_src = P->pair_src;
-  g.node_info = P->node_info;
-  g.node_ptr = P->node_ptr;
-  g.node_src = P->node_src;
-  g.p0 = g.p1 = g.n0 = g.n1 = 0;
-  g.ring_mask = W.ring_elems - 1;
+  const GatherArgs g = gather_args(P, W.ring_elems);
   QueueArgs Q;
   Q.tasks = reinterpret_cast<const int4*>(kWantK ? P->tasks_k : P->tasks_f);
   Q.n_tasks = (int32_t)(kWantK ? P->n_tasks_k : P->n_tasks_f);

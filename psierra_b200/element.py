@@ -200,3 +200,37 @@ class Tet4TotalLagrangian(_GPUElementBase):
         rho = self._material.mass_density
         m = np.kron(np.ones((4, 4)) + np.identity(4), np.identity(3))
         return (rho * volume / 20.0) * m
+
+
+# Exact reference mass matrix of the 10-node tetrahedron (entries / 2520), VTK ordering;
+# the consistent mass of psierra element/tet10_base.py:12-27, 344-372.
+_TET10_MASS_INT = np.array([
+    [36, 6, 6, 6, -24, -36, -24, -24, -36, -36],
+    [6, 36, 6, 6, -24, -24, -36, -36, -24, -36],
+    [6, 6, 36, 6, -36, -24, -24, -36, -36, -24],
+    [6, 6, 6, 36, -36, -36, -36, -24, -24, -24],
+    [-24, -24, -36, -36, 192, 96, 96, 96, 96, 48],
+    [-36, -24, -24, -36, 96, 192, 96, 48, 96, 96],
+    [-24, -36, -24, -36, 96, 96, 192, 96, 48, 96],
+    [-24, -36, -36, -24, 96, 48, 96, 192, 96, 96],
+    [-36, -24, -36, -24, 96, 96, 48, 96, 192, 96],
+    [-36, -36, -24, -24, 48, 96, 96, 96, 96, 192]], dtype=np.float64)
+
+
+class Tet10TotalLagrangian(_GPUElementBase):
+    """GPU Tet10 Total-Lagrangian element, 4-point rule (psierra ``element/tet10_total_lagrangian.py``)."""
+
+    _npe = 10
+
+    def __init__(self, material, default_quadrature_order: int = 4, precision: str = "fp64", device=None) -> None:
+        if default_quadrature_order != 4:
+            raise ValueError("the GPU Tet10 element integrates with the 4-point rule")
+        super().__init__(material, precision=precision, device=device)
+        self.default_quadrature_order = 4
+
+    def compute_mass_matrix(self, volume: float) -> np.ndarray:
+        rho = self._material.mass_density
+        return np.kron(_TET10_MASS_INT / 2520.0 * rho * volume, np.identity(3))
+
+    def assemble_mass_matrix(self, mesh):
+        raise NotImplementedError("the Tet10 consistent mass is assembled by SolidDomain.assemble_mass_matrix")

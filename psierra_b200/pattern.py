@@ -47,6 +47,7 @@ class MeshPattern:
         self._dev: dict | None = None
         self._blocks: tuple | None = None
         self._plan_host: dict | None = None
+        self.granule, self.tile, self.tile_items, self.lag = self.QUEUE[npe]
 
     @property
     def n_dofs(self) -> int:
@@ -64,9 +65,8 @@ class MeshPattern:
             self._blocks = (blk_ptr, blk_src)
         return self._blocks
 
-    GRANULE = 4096
-    TILE = 32
-    LAG = 8
+    # queue geometry per element type: granule (elements), element tile, item tile, lag (granules)
+    QUEUE = {4: (4096, 32, 32, 8), 10: (512, 8, 32, 16)}
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
@@ -78,7 +78,7 @@ class MeshPattern:
             check(L.psx_plan_count(ptr(self.conn), E, npe, N, ptr(self.nbr_ptr), ptr(n_pairs), ptr(n_src)),
                   "psx_plan_count")
             P, S = int(n_pairs[0]), int(n_src[0])
-            ng = (E + self.GRANULE - 1) // self.GRANULE
+            ng = (E + self.granule - 1) // self.granule
             h = {
                 "pair_info": np.zeros(4 * max(P, 1), dtype=np.int32),
                 "pair_ptr": np.zeros(P + 1, dtype=np.int32),
@@ -90,7 +90,7 @@ class MeshPattern:
                 "node_gptr": np.zeros(ng + 1, dtype=np.int32),
                 "max_span": np.zeros(1, dtype=np.int64),
             }
-            check(L.psx_plan_fill(ptr(self.conn), E, npe, N, ptr(self.nbr_ptr), ptr(self.nbr), self.GRANULE,
+            check(L.psx_plan_fill(ptr(self.conn), E, npe, N, ptr(self.nbr_ptr), ptr(self.nbr), self.granule,
                                   ptr(h["pair_info"]), ptr(h["pair_ptr"]), ptr(h["pair_src"]), ptr(h["pair_gptr"]),
                                   ptr(h["node_info"]), ptr(h["node_ptr"]), ptr(h["node_src"]), ptr(h["node_gptr"]),
                                   ptr(h["max_span"])), "psx_plan_fill")
@@ -120,20 +120,21 @@ class MeshPattern:
             st = _lib.PlanStruct()
             st.npe, st.n_granules = self.npe, h["n_granules"]
             st.n_elements, st.n_nodes, st.n_pairs = self.n_elements, self.n_nodes, h["n_pairs"]
-            st.granule, st.max_span = self.GRANULE, int(h["max_span"][0])
+            st.granule, st.max_span = self.granule, int(h["max_span"][0])
             for k in ("conn", "pair_info", "pair_ptr", "pair_src", "node_info", "node_ptr", "node_src"):
                 setattr(st, k, d[k].data_ptr())
             st.pair_gptr = h["pair_gptr"].ctypes.data
             st.node_gptr = h["node_gptr"].ctypes.data
-            st.tile, st.lag = self.TILE, self.LAG
+            st.tile, st.lag, st.tile_items = self.tile, self.lag, self.tile_items
             L = lib()
             for key, with_pairs in (("k", 1), ("f", 0)):
                 nt = ctypes.c_int64()
-                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.TILE, self.LAG, ctypes.byref(nt)),
-                      "psx_task_count")
+                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag,
+                                       ctypes.byref(nt)), "psx_task_count")
                 tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
                 btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
-                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.TILE, self.LAG, ptr(tasks), ptr(btiles)),
+                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag, ptr(tasks),
+                                      ptr(btiles)),
                       "psx_task_fill")
                 d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
                 setattr(st, "n_tasks_" + key, int(nt.value))

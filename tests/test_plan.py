@@ -79,9 +79,9 @@ def test_plan_gather_reproduces_coo_sum(name):
 def test_plan_granules_and_span():
     m = meshgen.box_tet4(1.0, 1.0, 1.0, 12, 10, 9)
     p = MeshPattern(m.elements, m.n_nodes)
-    p.GRANULE = 256
+    p.granule = 256
     h = p.plan_host()
-    g = p.GRANULE
+    g = p.granule
     span = int(h["max_span"][0])
     for q in range(h["n_pairs"]):
         es = h["pair_src"][h["pair_ptr"][q]:h["pair_ptr"][q + 1]] >> 6

@@ -26,14 +26,14 @@ def _queue(p: MeshPattern, with_pairs: int, tile: int, lag: int):
     st = _lib.PlanStruct()
     st.npe, st.n_granules = p.npe, h["n_granules"]
     st.n_elements, st.n_nodes, st.n_pairs = p.n_elements, p.n_nodes, h["n_pairs"]
-    st.granule, st.max_span = p.GRANULE, int(h["max_span"][0])
+    st.granule, st.max_span = p.granule, int(h["max_span"][0])
     st.pair_gptr, st.node_gptr = h["pair_gptr"].ctypes.data, h["node_gptr"].ctypes.data
     L = _lib.lib()
     nt = ctypes.c_int64()
-    _lib.check(L.psx_task_count(ctypes.byref(st), with_pairs, tile, lag, ctypes.byref(nt)), "count")
+    _lib.check(L.psx_task_count(ctypes.byref(st), with_pairs, tile, tile, lag, ctypes.byref(nt)), "count")
     tasks = np.zeros(4 * nt.value, dtype=np.int32)
     bt = np.zeros(h["n_granules"], dtype=np.int32)
-    _lib.check(L.psx_task_fill(ctypes.byref(st), with_pairs, tile, lag, _lib.ptr(tasks), _lib.ptr(bt)), "fill")
+    _lib.check(L.psx_task_fill(ctypes.byref(st), with_pairs, tile, tile, lag, _lib.ptr(tasks), _lib.ptr(bt)), "fill")
     return tasks.reshape(-1, 4), bt, h
 
 
@@ -42,7 +42,7 @@ def _queue(p: MeshPattern, with_pairs: int, tile: int, lag: int):
 def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
     m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
     p = MeshPattern(m.elements, m.n_nodes)
-    p.GRANULE = granule
+    p.granule = granule
     tile = 64
     tasks, bt, h = _queue(p, with_pairs, tile, lag)
     G = h["n_granules"]
