@@ -234,6 +234,18 @@ int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double* u,
                 void* stream);
 
 /*
+ * Vector-Jacobian product of the internal force (no counterpart in the reference, which
+ * is gradient-free): for a cotangent w (3N), gX_out (3N) = w^T df_int/dX, and, when not
+ * null, gmu_out / gkappa_out (E) = w^T df_int/dmu_e, w^T df_int/dkappa_e.  F is
+ * recomputed from (X, u); FP64 throughout; gX is gathered per node in fixed order.
+ * w^T df_int/du = K_T(u) w is psx_tet4_kv.  work as for psx_tet4_assemble (FP64).
+ */
+int psx_tet4_adjoint(const psx_plan_t* plan, const double* X, const double* u,
+                     const double* mu_e, const double* kappa_e, double mu, double kappa,
+                     const double* w, double* gX_out, double* gmu_out, double* gkappa_out,
+                     void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
  * One dynamic-relaxation pseudo-step on the linearised system K_T(u) x = b, fused into
  * a single pass (the viscous update of analysis/dynamic_relaxation.py:296-299,378-382):
  *   r = b - K_T(u) x,  a = minv * r,  vel = c1 vel + c2 a,  x += dt vel   (in place)
@@ -269,6 +281,14 @@ int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes);
 int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
             int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
             int precond, void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
+ * Symmetric elimination of prescribed DOFs in a CSR matrix, in place: rows and columns
+ * of DOFs with fixed[d] != 0 are zeroed and their diagonal set to 1 (the pattern and
+ * symmetry are kept).  fixed (device, n bytes).
+ */
+int psx_csr_dirichlet(int64_t n, const int32_t* indptr, const int32_t* indices, void* values,
+                      int value_precision, const uint8_t* fixed, void* stream);
 
 /*
  * psx_pcg without a workspace argument: no counterpart in the reference.  For callers

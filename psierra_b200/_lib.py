@@ -59,6 +59,8 @@ SIGNATURES: dict[str, list] = {
     "psx_tet10_assemble": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _i32, _i32, _p, _p, _p, _i64, _p, _p],
     "psx_tet10_element_dets": [_p, _p, _p, _i64, _p, _p],
     "psx_pcg_work_bytes": [_i64, _i32, _p],
+    "psx_csr_dirichlet": [_i64, _p, _p, _p, _i32, _p, _p],
+    "psx_tet4_adjoint": [_p, _p, _p, _p, _p, _f64, _f64, _p, _p, _p, _p, _p, _i64, _p, _p],
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
 }
 

@@ -168,6 +168,25 @@ class GPUAssembler:
             self.raise_on_bad_elements(u)
         return y_out
 
+    def adjoint(self, u: torch.Tensor, w: torch.Tensor, want_params: bool = True):
+        """Vector-Jacobian product of f_int: ``(gX (3N), gmu (E), gkappa (E))`` for cotangent ``w``.
+
+        FP64; F is recomputed from (X, u).  ``w^T df/du`` is ``kv(u, w)`` (K_T is symmetric).
+        """
+        u = self._check_u(u)
+        w = self._check_u(w)
+        gX = self.new_f()
+        gmu = torch.empty(self.n_elements, dtype=torch.float64, device=self.device) if want_params else None
+        gk = torch.empty(self.n_elements, dtype=torch.float64, device=self.device) if want_params else None
+        self.status.zero_()
+        work = self.workspace("fp64")
+        check(lib().psx_tet4_adjoint(ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u), ptr(self.mu_e),
+                                     ptr(self.kappa_e), self.mu, self.kappa, ptr(w), ptr(gX), ptr(gmu), ptr(gk),
+                                     ptr(work), work.numel(), ptr(self.status), _stream_handle()),
+              "psx_tet4_adjoint")
+        self.raise_on_bad_elements(u)
+        return gX, gmu, gk
+
     def dr_step(self, u: torch.Tensor, b: torch.Tensor, minv: torch.Tensor, x: torch.Tensor, vel: torch.Tensor,
                 c1: float, c2: float, dt: float, precision: str | None = None,
                 r_out: torch.Tensor | None = None) -> None:

@@ -62,6 +62,7 @@ struct PointState {
   double Finv[3][3];  // F^-1
   double P[3][3];     // first Piola-Kirchhoff stress F S
   double Jm1;         // J - 1 (compensated)
+  double lnJ;         // ln J
   double phi;         // mu J^(-2/3)
   double beta;        // kappa ln J
   double I1;          // tr C
@@ -78,7 +79,8 @@ __device__ __forceinline__ void neohookean_point(const double l[3][3], double mu
 #pragma unroll
     for (int k = 0; k < 3; ++k) trl2 += l[i][k] * l[k][i];
   s.Jm1 = trl + 0.5 * (trl * trl - trl2) + det3(l);
-  double lnJ = log1p(s.Jm1);
+  const double lnJ = log1p(s.Jm1);
+  s.lnJ = lnJ;
   s.phi = mu * exp((-2.0 / 3.0) * lnJ);
   s.beta = kappa * lnJ;
 #pragma unroll

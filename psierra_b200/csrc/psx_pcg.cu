@@ -403,6 +403,43 @@ extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices,
 }
 
 // ---------------------------------------------------------------------------------------
+// Symmetric elimination of prescribed DOFs in a CSR matrix (in place): rows and columns
+// of fixed DOFs are zeroed and their diagonal set to 1, which keeps the matrix symmetric
+// positive definite and its pattern (and node alignment) unchanged.
+namespace {
+template <typename VT>
+__global__ void csr_dirichlet_kernel(int64_t n, const int32_t* __restrict__ indptr,
+                                     const int32_t* __restrict__ indices, VT* __restrict__ vals,
+                                     const uint8_t* __restrict__ fixed) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const bool fr = fixed[r] != 0;
+    for (int32_t j = indptr[r]; j < indptr[r + 1]; ++j) {
+      const int32_t c = indices[j];
+      if (fr)
+        vals[j] = (c == r) ? (VT)1 : (VT)0;
+      else if (fixed[c])
+        vals[j] = (VT)0;
+    }
+  }
+}
+}  // namespace
+
+extern "C" int psx_csr_dirichlet(int64_t n, const int32_t* indptr, const int32_t* indices, void* values,
+                                 int value_precision, const uint8_t* fixed, void* stream) {
+  if (n <= 0 || !indptr || !indices || !values || !fixed) return PSX_ERR_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int grid = (int)std::min<int64_t>(148 * 8, (n + 255) / 256);
+  if (value_precision == PSX_FP64)
+    psx::csr_dirichlet_kernel<double><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<double*>(values), fixed);
+  else if (value_precision == PSX_FP32_MIXED)
+    psx::csr_dirichlet_kernel<float><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<float*>(values), fixed);
+  else
+    return PSX_ERR_ARG;
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 // Allocation-free variant: psx_pcg_static.
 //
 // Some callers cannot hand this library a workspace.  A host code that owns all device

@@ -28,7 +28,8 @@ namespace psx {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr int kModeDR = 16;  // internal: PSX_KV with the fused dynamic-relaxation epilogue
+constexpr int kModeDR = 16;       // internal: PSX_KV with the fused dynamic-relaxation epilogue
+constexpr int kModeAdjoint = 64;  // internal: vector-Jacobian product of f_int
 #ifndef PSX_TET4_MIN_BLOCKS
 #define PSX_TET4_MIN_BLOCKS 2
 #endif
@@ -87,7 +88,9 @@ struct Tet4Args {
   const int32_t* conn;
   const double* X;
   const double* U;
-  const double* Vv;  // vector of the matrix-free product (PSX_KV)
+  const double* Vv;  // vector of the matrix-free product (PSX_KV) / cotangent (adjoint)
+  double* dmu;       // adjoint: d(w.f)/d mu_e (E), or null
+  double* dkappa;    // adjoint: d(w.f)/d kappa_e (E), or null
   const double* mu_e;
   const double* kappa_e;
   double mu0, kappa0, lam0;
@@ -102,7 +105,8 @@ template <typename KT, int MODE, bool KGLOBAL = true>
 __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
                                              double* __restrict__ frec) {
   using L = RecLayout<4>;
-  constexpr bool kKV = (MODE & PSX_KV) != 0;
+  constexpr bool kAdj = (MODE & kModeAdjoint) != 0;
+  constexpr bool kKV = (MODE & PSX_KV) != 0 || kAdj;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 && !kKV;
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
   constexpr bool kMass = (MODE & PSX_MASS) != 0;
@@ -127,6 +131,8 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   KT p[4][3], q[4][3];
   TangentCoef<KT> tc;
   KT gk[4][3];
+  // copies kept for the adjoint branch (dead code otherwise)
+  double ps_F[3][3], ps_Finv[3][3], ps_P[3][3], ps_lnJ = 0.0, Un_[4][3], l_[3][3];
 #pragma unroll
   for (int b = 0; b < 4; ++b)
 #pragma unroll
@@ -150,6 +156,22 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     PointState ps;
     neohookean_point(l, mu, kappa, ps);
     if (G.detD > 0.0 && ps.Jm1 <= -1.0) flag_bad_element(A.st, e, false);
+    if constexpr (kAdj) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          ps_F[i][j] = ps.F[i][j];
+          ps_Finv[i][j] = ps.Finv[i][j];
+          ps_P[i][j] = ps.P[i][j];
+          l_[i][j] = l[i][j];
+        }
+      ps_lnJ = ps.lnJ;
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Un_[b][k] = Un[b][k];
+    }
     if constexpr (kWantF) {
       double fr[12];
 #pragma unroll
@@ -217,15 +239,113 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
       }
     }
     double yr[12];
+    if constexpr (!kAdj) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        KT t = alpha * p[a][k] + beta * tc.c * q[a][k];
+        for (int k = 0; k < 3; ++k) {
+          KT t = alpha * p[a][k] + beta * tc.c * q[a][k];
 #pragma unroll
-        for (int m = 0; m < 3; ++m) t += Pv[k][m] * (tc.hb * p[a][m]) + tc.phi * gk[a][m] * Gv[m][k];
-        yr[3 * a + k] = (double)t;
+          for (int m = 0; m < 3; ++m) t += Pv[k][m] * (tc.hb * p[a][m]) + tc.phi * gk[a][m] * Gv[m][k];
+          yr[3 * a + k] = (double)t;
+        }
+    } else {
+      // Vector-Jacobian product of w.f_e with f_e,a = V P g_a (the adjoint of
+      // tet4_total_lagrangian.py:136-137 w.r.t. X, mu, kappa).  L_w = sum_b w_b g_b^T,
+      // VM = V dP/dF[L_w] = alpha F^-T + hb Pv F^-T + beta c F + phi Gv^T.
+      double Fi[3][3], Fm[3][3], VM[3][3], Lw[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          Fi[i][j] = (double)ps_Finv[i][j];
+          Fm[i][j] = (double)ps_F[i][j];
+          Lw[i][j] = 0.0;
+        }
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) Lw[i][j] += Vn[b][i] * G.g[b][j];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          // (F^-T)[k][m] = Finv[m][k]
+          double t = (double)alpha * Fi[m][k] + (double)beta * (double)tc.c * Fm[k][m] + (double)tc.phi * (double)Gv[m][k];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) t += (double)Pv[k][j] * (double)tc.hb * Fi[m][j];
+          VM[k][m] = t;
+        }
+      // h_b = VM^T u_b + V P^T w_b  (vectors conjugate to dg_b)
+      double h[4][3];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          double t = 0.0;
+#pragma unroll
+          for (int i = 0; i < 3; ++i) t += VM[i][j] * Un_[b][i] + G.V * ps_P[i][j] * Vn[b][i];
+          h[b][j] = t;
+        }
+      double PL = 0.0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) PL += ps_P[i][j] * Lw[i][j];
+      // dL/dD = PL V G^T - G^T Hm G^T with G = D^-1 (rows g_1..g_3), Hm rows h_b - h_0
+      double Gm[3][3], Hm[3][3], T1[3][3], Z[3][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          Gm[r][j] = G.g[r + 1][j];
+          Hm[r][j] = h[r + 1][j] - h[0][j];
+        }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)  // T1 = G^T Hm
+#pragma unroll
+        for (int j = 0; j < 3; ++j) T1[i][j] = Gm[0][i] * Hm[0][j] + Gm[1][i] * Hm[1][j] + Gm[2][i] * Hm[2][j];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          Z[i][j] = PL * G.V * Gm[j][i] - (T1[i][0] * Gm[j][0] + T1[i][1] * Gm[j][1] + T1[i][2] * Gm[j][2]);
+      // D[i][j] = X_{j+1}[i] - X_0[i]
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        yr[i] = -(Z[i][0] + Z[i][1] + Z[i][2]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) yr[3 * (j + 1) + i] = Z[i][j];
       }
+      // parameter gradients: dP/dmu = 2 J^-2/3 F^-T dev E, dP/dkappa = ln J F^-T
+      if (A.dmu || A.dkappa) {
+        double E[3][3], trE = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double ltl = l_[0][i] * l_[0][j] + l_[1][i] * l_[1][j] + l_[2][i] * l_[2][j];
+            E[i][j] = 0.5 * (l_[i][j] + l_[j][i] + ltl);
+          }
+        trE = E[0][0] + E[1][1] + E[2][2];
+        const double jm23 = exp((-2.0 / 3.0) * ps_lnJ);
+        double FTL = 0.0, FDL = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            FTL += Fi[j][i] * Lw[i][j];
+            double fd = 0.0;  // (F^-T dev E)[i][j]
+#pragma unroll
+            for (int k = 0; k < 3; ++k) fd += Fi[k][i] * (E[k][j] - (k == j ? trE / 3.0 : 0.0));
+            FDL += fd * Lw[i][j];
+          }
+        if (A.dmu) A.dmu[e] = G.V * 2.0 * jm23 * FDL;
+        if (A.dkappa) A.dkappa[e] = G.V * ps_lnJ * FTL;
+      }
+    }
     double2* fq = reinterpret_cast<double2*>(frec);
 #pragma unroll
     for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(yr[2 * i], yr[2 * i + 1]));
@@ -287,7 +407,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
                        KT* __restrict__ k_out, double* __restrict__ f_out, DRArgs dr) {
   using L = RecLayout<4>;
-  constexpr bool kKV = (MODE & PSX_KV) != 0;
+  constexpr bool kKV = (MODE & (PSX_KV | kModeAdjoint)) != 0;
   constexpr bool kDR = (MODE & kModeDR) != 0;
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && !kKV;
@@ -345,7 +465,8 @@ __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double*
 template <typename KT, int MODE>
 int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
              cudaStream_t stream, const DRArgs& dr = DRArgs{}) {
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && (MODE & PSX_KV) == 0;
+  constexpr bool kWantK =
+      (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && (MODE & (PSX_KV | kModeAdjoint)) == 0;
   const GatherArgs g = gather_args(P, W.ring_elems);
   QueueArgs Q;
   Q.tasks = reinterpret_cast<const int4*>(kWantK ? P->tasks_k : P->tasks_f);
@@ -403,7 +524,7 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   int rc = work_layout(plan, precision, work, &W, kMinBlocks);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
-  Tet4Args A{plan->conn, X, u, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
+  Tet4Args A{plan->conn, X, u, nullptr, nullptr, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define PSX_T4(KT, M) run_tet4<KT, M>(plan, A, W, static_cast<KT*>(k_out), f_out, s)
   if (mass) return precision == PSX_FP64 ? PSX_T4(double, PSX_MASS) : PSX_T4(float, PSX_MASS);
@@ -424,7 +545,7 @@ extern "C" int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double
   int rc = work_layout(plan, precision, work, &W, kMinBlocks);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
-  Tet4Args A{plan->conn, X, u, v, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
+  Tet4Args A{plan->conn, X, u, v, nullptr, nullptr, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   return precision == PSX_FP64 ? run_tet4<double, PSX_KV>(plan, A, W, nullptr, y_out, s)
                                : run_tet4<float, PSX_KV>(plan, A, W, nullptr, y_out, s);
@@ -440,11 +561,25 @@ extern "C" int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const d
   int rc = work_layout(plan, precision, work, &W, kMinBlocks);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
-  Tet4Args A{plan->conn, X, u, x, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
+  Tet4Args A{plan->conn, X, u, x, nullptr, nullptr, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
   DRArgs dr{b, minv, c1, c2, dt, x, vel};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   return precision == PSX_FP64 ? run_tet4<double, PSX_KV | kModeDR>(plan, A, W, nullptr, r_out, s, dr)
                                : run_tet4<float, PSX_KV | kModeDR>(plan, A, W, nullptr, r_out, s, dr);
+}
+
+extern "C" int psx_tet4_adjoint(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
+                                const double* kappa_e, double mu, double kappa, const double* w, double* gX_out,
+                                double* gmu_out, double* gkappa_out, void* work, int64_t work_bytes, void* status,
+                                void* stream) {
+  using namespace psx;
+  if (!plan || plan->npe != 4 || !X || !u || !w || !gX_out || !status || !work) return PSX_ERR_ARG;
+  WorkLayout W;
+  int rc = work_layout(plan, PSX_FP64, work, &W, kMinBlocks);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
+  Tet4Args A{plan->conn, X, u, w, gmu_out, gkappa_out, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
+  return run_tet4<double, kModeAdjoint>(plan, A, W, nullptr, gX_out, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int psx_tet4_element_dets(const int32_t* conn, const double* X, const double* u, int64_t e,

@@ -1,0 +1,108 @@
+"""Adjoint gradients against central finite differences (GPU).
+
+Tolerance: 1e-5 relative (the north-star bound for adjoint gradients vs FD).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel_2
+from psierra_b200 import meshgen
+from psierra_b200.adjoint import internal_force, static_equilibrium
+from psierra_b200.assembler import GPUAssembler
+from psierra_b200.material import NeoHookeanField
+from psierra_b200.newton import DeviceNewton
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda")
+
+
+def problem(seed=0, cells=(3, 2, 2)):
+    m = meshgen.box_tet4(1.0, 0.4, 0.3, *cells)
+    rng = np.random.default_rng(seed)
+    mu = np.exp(np.log(1000.0) + 0.3 * rng.normal(size=m.n_elements))
+    kappa = 50.0 * mu
+    asm = GPUAssembler(m.nodes, m.elements, NeoHookeanField(mu, kappa))
+    return m, asm, mu, kappa, rng
+
+
+def test_internal_force_vjp_matches_central_differences():
+    m, asm, mu, kappa, rng = problem()
+    X = torch.from_numpy(m.nodes.copy()).to(DEV).requires_grad_(True)
+    u = torch.from_numpy(0.03 * rng.normal(size=(m.n_nodes, 3))).to(DEV).requires_grad_(True)
+    mu_t = torch.from_numpy(mu).to(DEV).requires_grad_(True)
+    ka_t = torch.from_numpy(kappa).to(DEV).requires_grad_(True)
+    w = torch.from_numpy(rng.normal(size=m.n_dofs)).to(DEV)
+    f = internal_force(asm, X, u, mu_t, ka_t)
+    (f @ w).backward()
+
+    def F(Xn, un, mun, kan):
+        with torch.no_grad():
+            return float(internal_force(asm, Xn, un, mun, kan) @ w)
+
+    h = 1e-6
+    for name, t, scale in (("X", X, 1.0), ("u", u, 1.0), ("mu", mu_t, 1000.0), ("kappa", ka_t, 50000.0)):
+        g = t.grad.detach().reshape(-1)
+        idx = rng.choice(g.numel(), size=8, replace=False)
+        fd = []
+        for i in idx:
+            args = [X.detach().clone(), u.detach().clone(), mu_t.detach().clone(), ka_t.detach().clone()]
+            k = ("X", "u", "mu", "kappa").index(name)
+            step = h * scale
+            args[k].view(-1)[i] += step
+            fp = F(*args)
+            args[k].view(-1)[i] -= 2 * step
+            fm = F(*args)
+            fd.append((fp - fm) / (2 * step))
+        fd = np.array(fd)
+        got = g[torch.as_tensor(idx, device=DEV)].cpu().numpy()
+        assert np.abs(got - fd).max() <= 1e-5 * np.abs(fd).max() + 1e-12, name
+
+
+def test_static_equilibrium_gradient_matches_central_differences():
+    m, asm, mu, kappa, rng = problem(seed=3, cells=(6, 2, 2))
+    clamp = meshgen.nodes_on_plane(m, 0, "min")
+    fixed = np.concatenate([3 * clamp + c for c in range(3)])
+    nt = DeviceNewton(asm, fixed, precision="fp64", pcg_tol=1e-13)
+    f_ext = torch.from_numpy(meshgen.traction_nodal_forces(m, 0, "max", [0.0, 0.0, -40.0])).to(DEV)
+    obs = np.arange(m.n_dofs)[2::3]
+    tgt = torch.zeros(len(obs), dtype=torch.float64, device=DEV)
+    obs_t = torch.from_numpy(obs).to(DEV)
+
+    def loss_of(mu_np):
+        mt = torch.from_numpy(mu_np).to(DEV).requires_grad_(True)
+        u = static_equilibrium(nt, mt, 50.0 * mt, f_ext, n_steps=2, nr_tol=1e-13)
+        L = 0.5 * torch.sum((u[obs_t] - tgt) ** 2)
+        return L, mt
+
+    L, mt = loss_of(mu)
+    L.backward()
+    g = mt.grad.cpu().numpy()
+    for e in rng.choice(m.n_elements, size=8, replace=False):
+        h = 1e-6 * mu[e]
+        mp, mm = mu.copy(), mu.copy()
+        mp[e] += h
+        mm[e] -= h
+        with torch.no_grad():
+            fd = (float(loss_of(mp)[0]) - float(loss_of(mm)[0])) / (2 * h)
+        assert abs(g[e] - fd) <= 1e-5 * abs(fd) + 1e-14 * abs(float(L)), (e, g[e], fd)
+
+
+def test_device_newton_matches_reference_beam():
+    g = golden("newton_beam")
+    mb = meshgen.box_tet4(1.0, 0.1, 0.1, 10, 2, 2)
+    mu, kappa = float(g["mu"]), float(g["kappa"])
+    E = mb.n_elements
+    asm = GPUAssembler(mb.nodes, mb.elements, NeoHookeanField(np.full(E, mu), np.full(E, kappa)))
+    fixed = np.concatenate([3 * g["clamp"] + c for c in range(3)])
+    nt = DeviceNewton(asm, fixed, precision="fp64", pcg_tol=1e-13)
+    res = nt.solve(torch.from_numpy(g["f_ext"]).to(DEV), n_steps=4, nr_iterations=25, nr_tol=1e-8)
+    assert res.converged
+    assert rel_2(res.u.cpu().numpy(), g["u"]) < 1e-8
+    # the FP32-mixed tangent converges to the same FP64 equilibrium
+    nt32 = DeviceNewton(asm, fixed, precision="fp32-mixed", pcg_tol=1e-10)
+    r32 = nt32.solve(torch.from_numpy(g["f_ext"]).to(DEV), n_steps=4, nr_iterations=40, nr_tol=1e-8)
+    assert r32.converged
+    assert rel_2(r32.u.cpu().numpy(), g["u"]) < 1e-7
