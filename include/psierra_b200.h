@@ -137,7 +137,7 @@ typedef struct psx_plan {
   int32_t tile;             /* elements per element task (psx_task_fill) */
   int32_t lag;              /* granules between an element tile and the gathers it completes */
   int32_t tile_items;       /* items per gather task */
-  int32_t pad_;
+  int32_t blocks_per_sm;    /* persistent blocks launched per SM; 0 = the kernel's register target */
   int64_t n_tasks_k;        /* task queue with pair tiles (any request involving K) */
   int64_t n_tasks_f;        /* task queue without pair tiles (f only) */
   const int32_t* tasks_k;   /* device, 4 per task: kind, granule, begin, end */
@@ -281,6 +281,24 @@ int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes);
 int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
             int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
             int precond, void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
+ * psx_pcg with a fixed trip count and no host synchronisation (no counterpart in the
+ * reference, whose solves always return to Python): exactly maxiter iterations are
+ * enqueued on the stream and become no-ops once converged, so the call can be captured
+ * in a CUDA graph.  Same arguments, results and status as psx_pcg.
+ */
+int psx_pcg_enqueue(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                    int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+                    int precond, void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
+ * out[s] = sum of x[i]^2 for offsets[s] <= i < offsets[s+1] (device arrays; offsets int64,
+ * n_seg + 1 entries), reduced in a fixed order: the per-mesh residual norms of a batch of
+ * meshes stored back to back (the per-instance ||R_free|| test of
+ * analysis/nonlinear_static.py:321-345 for every mesh at once).
+ */
+int psx_segment_sumsq(int64_t n_seg, const int64_t* offsets, const double* x, double* out, void* stream);
 
 /*
  * Symmetric elimination of prescribed DOFs in a CSR matrix, in place: rows and columns

@@ -62,6 +62,8 @@ SIGNATURES: dict[str, list] = {
     "psx_csr_dirichlet": [_i64, _p, _p, _p, _i32, _p, _p],
     "psx_tet4_adjoint": [_p, _p, _p, _p, _p, _f64, _f64, _p, _p, _p, _p, _p, _i64, _p, _p],
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
+    "psx_pcg_enqueue": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
+    "psx_segment_sumsq": [_i64, _p, _p, _p, _p],
 }
 
 
@@ -89,7 +91,7 @@ class PlanStruct(ctypes.Structure):
         ("tile", ctypes.c_int32),
         ("lag", ctypes.c_int32),
         ("tile_items", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("blocks_per_sm", ctypes.c_int32),
         ("n_tasks_k", ctypes.c_int64),
         ("n_tasks_f", ctypes.c_int64),
         ("tasks_k", ctypes.c_void_p),

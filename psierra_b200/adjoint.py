@@ -59,10 +59,10 @@ def internal_force(asm: GPUAssembler, X, u, mu_e, kappa_e):
 
 class StaticEquilibrium(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, mu_e, kappa_e, f_ext, newton: DeviceNewton, n_steps: int, nr_tol: float):
+    def forward(ctx, mu_e, kappa_e, f_ext, newton: DeviceNewton, n_steps: int, nr_tol: float, polish: int):
         asm = newton.asm
         _set_params(asm, None, mu_e, kappa_e)
-        res = newton.solve(f_ext.detach(), n_steps=n_steps, nr_tol=nr_tol)
+        res = newton.solve(f_ext.detach(), n_steps=n_steps, nr_tol=nr_tol, polish=polish)
         if not res.converged:
             raise RuntimeError("static equilibrium did not converge")
         ctx.newton = newton
@@ -78,11 +78,13 @@ class StaticEquilibrium(torch.autograd.Function):
         rhs = torch.where(nt.free, gu.detach(), torch.zeros_like(gu))
         lam, _ = nt.solve_linear(rhs)
         _, gmu, gk = nt.asm.adjoint(u, lam)
-        return -gmu, -gk, lam, None, None, None
+        return -gmu, -gk, lam, None, None, None, None
 
 
-def static_equilibrium(newton: DeviceNewton, mu_e, kappa_e, f_ext, n_steps: int = 1, nr_tol: float = 1e-12):
-    return StaticEquilibrium.apply(mu_e, kappa_e, f_ext, newton, n_steps, nr_tol)
+def static_equilibrium(newton: DeviceNewton, mu_e, kappa_e, f_ext, n_steps: int = 1, nr_tol: float = 1e-10,
+                       polish: int = 2):
+    """u*(mu_e, kappa_e, f_ext) with an adjoint backward; ``polish`` as in ``DeviceNewton.solve``."""
+    return StaticEquilibrium.apply(mu_e, kappa_e, f_ext, newton, n_steps, nr_tol, polish)
 
 
 def identify_shear_moduli(newton: DeviceNewton, f_ext, obs_dofs, u_target, mu0, kappa_ratio: float = 50.0,

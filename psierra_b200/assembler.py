@@ -94,6 +94,13 @@ class GPUAssembler:
         """Kernel launches one assemble() call makes (one persistent kernel)."""
         return 1
 
+    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None) -> None:
+        """Launch shape of the persistent kernel (see ``MeshPattern.set_queue``)."""
+        old = self.pattern.lag
+        self.pattern.set_queue(lag=lag, blocks_per_sm=blocks_per_sm)
+        if self.pattern.lag != old:
+            self._work.clear()  # the record ring is sized by the lag
+
     def workspace(self, precision: str) -> torch.Tensor:
         w = self._work.get(precision)
         if w is None:

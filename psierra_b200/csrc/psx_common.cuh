@@ -167,6 +167,20 @@ __device__ __forceinline__ void flag_bad_element(Status* st, int64_t e, bool vol
   atomicMax(&st->first_bad_key, (int32_t)(0x7fffffff - (int32_t)e));
 }
 
+// Raise a kernel's dynamic shared-memory limit once per device, so that later launches
+// (including launches captured into a CUDA graph) make no attribute call.
+template <typename K>
+inline cudaError_t set_dynamic_smem_once(K* kernel, int bytes, unsigned long long* done_mask) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (__atomic_load_n(done_mask, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) __atomic_fetch_or(done_mask, bit, __ATOMIC_RELEASE);
+  return e;
+}
+
 }  // namespace psx
 
 #define PSX_CUDA_CHECK_LAUNCH()                      \

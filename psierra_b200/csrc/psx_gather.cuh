@@ -395,7 +395,10 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   const int sms = device_sm_count();
   if (sms <= 0) return PSX_ERR_CUDA;
   const int64_t ntask = P->n_tasks_k > P->n_tasks_f ? P->n_tasks_k : P->n_tasks_f;
-  W->grid = (int32_t)(sms * blocks_per_sm < ntask ? sms * blocks_per_sm : ntask);
+  // a plan may override the blocks per SM (the autotuner's knob); tasks are claimed in
+  // queue order, so any grid is deadlock-free and extra blocks only queue for an SM
+  const int bps = P->blocks_per_sm > 0 ? (P->blocks_per_sm < 4 ? P->blocks_per_sm : 4) : blocks_per_sm;
+  W->grid = (int32_t)(sms * bps < ntask ? sms * bps : ntask);
   auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
   W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
   const int64_t kbytes = up(W->ring_elems * kK * kt);

@@ -331,7 +331,7 @@ int layout(int64_t n, int precond, void* work, PcgWork* w, int64_t* bytes) {
 template <typename VT, bool BLOCK>
 int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* vals, const double* b, double* x,
             double rtol, double atol, int32_t maxiter, const PcgWork& w, Status* st, cudaStream_t s,
-            int identity) {
+            int identity, bool host_checks) {
   const int grid_vec = (int)std::min<int64_t>(kGridMax, (n + kBlock - 1) / kBlock);
   const int grid_row = (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
   if (cudaMemsetAsync(w.s, 0, sizeof(PcgScalars), s) != cudaSuccess) return PSX_ERR_CUDA;
@@ -355,6 +355,7 @@ int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* 
     }
     PSX_CUDA_CHECK_LAUNCH();
     done += batch;
+    if (!host_checks) continue;  // fixed trip count, nothing read back (stream-capturable)
     if (cudaMemcpyAsync(&host, w.s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess)
       return PSX_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return PSX_ERR_CUDA;
@@ -375,9 +376,10 @@ extern "C" int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes) {
   return psx::layout(n, precond, nullptr, &w, bytes);
 }
 
-extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
-                       int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
-                       int precond, void* work, int64_t work_bytes, void* status, void* stream) {
+namespace {
+int pcg_entry(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values, int value_precision,
+              const double* b, double* x, double rtol, double atol, int32_t maxiter, int precond, void* work,
+              int64_t work_bytes, void* status, void* stream, bool host_checks) {
   using namespace psx;
   if (n <= 0 || !indptr || !indices || !values || !b || !x || !work || !status || maxiter < 0) return PSX_ERR_ARG;
   if (precond < PSX_PRECOND_NONE || precond > PSX_PRECOND_BJACOBI) return PSX_ERR_ARG;
@@ -394,12 +396,28 @@ extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices,
   const int id = precond == PSX_PRECOND_NONE;
   if (value_precision == PSX_FP64) {
     const double* v = static_cast<const double*>(values);
-    return blk ? run_pcg<double, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id)
-               : run_pcg<double, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id);
+    return blk ? run_pcg<double, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks)
+               : run_pcg<double, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks);
   }
   const float* v = static_cast<const float*>(values);
-  return blk ? run_pcg<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id)
-             : run_pcg<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id);
+  return blk ? run_pcg<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks)
+             : run_pcg<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks);
+}
+}  // namespace
+
+extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                       int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+                       int precond, void* work, int64_t work_bytes, void* status, void* stream) {
+  return pcg_entry(n, indptr, indices, values, value_precision, b, x, rtol, atol, maxiter, precond, work, work_bytes,
+                   status, stream, true);
+}
+
+extern "C" int psx_pcg_enqueue(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                               int value_precision, const double* b, double* x, double rtol, double atol,
+                               int32_t maxiter, int precond, void* work, int64_t work_bytes, void* status,
+                               void* stream) {
+  return pcg_entry(n, indptr, indices, values, value_precision, b, x, rtol, atol, maxiter, precond, work, work_bytes,
+                   status, stream, false);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -430,11 +448,36 @@ extern "C" int psx_csr_dirichlet(int64_t n, const int32_t* indptr, const int32_t
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int grid = (int)std::min<int64_t>(148 * 8, (n + 255) / 256);
   if (value_precision == PSX_FP64)
-    psx::csr_dirichlet_kernel<double><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<double*>(values), fixed);
+    csr_dirichlet_kernel<double><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<double*>(values), fixed);
   else if (value_precision == PSX_FP32_MIXED)
-    psx::csr_dirichlet_kernel<float><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<float*>(values), fixed);
+    csr_dirichlet_kernel<float><<<grid, 256, 0, s>>>(n, indptr, indices, static_cast<float*>(values), fixed);
   else
     return PSX_ERR_ARG;
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-segment sums of squares (one block per segment, fixed reduction tree): the residual
+// norms of the meshes of a batch, whose DOFs occupy contiguous ranges of one vector.
+namespace {
+__global__ void __launch_bounds__(psx::kBlock) segment_sumsq_kernel(int64_t n_seg, const int64_t* __restrict__ offsets,
+                                                                     const double* __restrict__ x,
+                                                                     double* __restrict__ out) {
+  for (int64_t sgi = blockIdx.x; sgi < n_seg; sgi += gridDim.x) {
+    const int64_t lo = offsets[sgi], hi = offsets[sgi + 1];
+    double v[1] = {0.0};
+    for (int64_t i = lo + threadIdx.x; i < hi; i += psx::kBlock) v[0] += x[i] * x[i];
+    psx::block_sum<1>(v);
+    if (threadIdx.x == 0) out[sgi] = v[0];
+  }
+}
+}  // namespace
+
+extern "C" int psx_segment_sumsq(int64_t n_seg, const int64_t* offsets, const double* x, double* out, void* stream) {
+  if (n_seg <= 0 || !offsets || !x || !out) return PSX_ERR_ARG;
+  const int grid = (int)std::min<int64_t>(n_seg, 148 * 8);
+  segment_sumsq_kernel<<<grid, psx::kBlock, 0, static_cast<cudaStream_t>(stream)>>>(n_seg, offsets, x, out);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }

@@ -322,8 +322,8 @@ int run_tet10(const psx_plan_t* P, const Tet10Args& A, const WorkLayout& W, KT* 
   Q.n_elements = P->n_elements;
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
   const size_t smem = sizeof(Tet10Smem<KT>) * (kThreads10 / 32);
-  if (cudaFuncSetAttribute(tet10_persistent_kernel<KT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+  static unsigned long long s_smem_set = 0;
+  if (set_dynamic_smem_once(tet10_persistent_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess)
     return PSX_ERR_CUDA;
   tet10_persistent_kernel<KT, MODE><<<W.grid, kThreads10, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec),
                                                                           W.frec, k_out, f_out);

@@ -482,9 +482,8 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
   constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
   const size_t smem = kStage ? sizeof(float) * (kThreads / 32) * StageSmem<KT>::kWarpFloats : 0;
-  if (smem > 0 &&
-      cudaFuncSetAttribute(tet4_persistent_kernel<KT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+  static unsigned long long s_smem_set = 0;
+  if (smem > 0 && set_dynamic_smem_once(tet4_persistent_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess)
     return PSX_ERR_CUDA;
   tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
                                                                       k_out, f_out, dr);

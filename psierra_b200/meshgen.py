@@ -197,3 +197,77 @@ def nodes_on_plane(mesh: TetMesh, axis: int, bound: str, tol: float = 1e-4) -> n
     c = mesh.nodes[:, axis]
     target = c.min() if bound == "min" else c.max()
     return np.where(np.abs(c - target) <= tol)[0].astype(np.int64)
+
+
+# ---------------------------------------------------------------------------
+# Batches of meshes
+# ---------------------------------------------------------------------------
+
+def concat_meshes(meshes) -> tuple[TetMesh, np.ndarray, np.ndarray]:
+    """Disjoint union of meshes: ``(union, node_offsets, element_offsets)`` (offsets B+1).
+
+    Instance ``i`` owns nodes ``node_offsets[i]:node_offsets[i+1]`` and elements
+    ``element_offsets[i]:element_offsets[i+1]`` of the union, in its own order.
+    """
+    nn = np.array([m.n_nodes for m in meshes], dtype=np.int64)
+    ne = np.array([m.n_elements for m in meshes], dtype=np.int64)
+    node_off = np.concatenate([[0], np.cumsum(nn)])
+    elem_off = np.concatenate([[0], np.cumsum(ne)])
+    nodes = np.concatenate([np.asarray(m.nodes, dtype=np.float64) for m in meshes])
+    elements = np.concatenate([np.asarray(m.elements, dtype=np.int64) + node_off[i] for i, m in enumerate(meshes)])
+    return TetMesh(nodes, elements), node_off, elem_off
+
+
+@dataclass
+class BeamCase:
+    mesh: TetMesh
+    length: float
+    youngs: float
+    poisson: float
+    traction: np.ndarray  # (3,) Pa on the x = length face
+    cells: tuple
+
+
+def beam_batch(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, section: float = 0.1) -> list[BeamCase]:
+    """Seeded batch of clamped cantilever beams of uneven size.
+
+    Length L ~ U[0.5, 2], square section ``section`` x ``section``; cell counts follow
+    one seeded size variable s ~ U[0, 1] per beam, (nx, ny, nz) = (8 + 112 s^p,
+    2 + 8 s^p, 2 + 8 s^p) rounded, with the exponent p chosen so that the batch holds
+    about ``target_tets`` tetrahedra (6 per cell) within the [8x2x2, 120x10x10] range.
+    E ~ U[1e3, 1e6] Pa, nu ~ U[0.3, 0.49], traction magnitude |t| ~ U[10, 1000] Pa on
+    the tip face: |t| along +x (tension) plus a transverse -z part of min(|t|/2,
+    E / (1600 L^2)), which keeps the linear tip-deflection estimate 400 t_z L^2 / E of
+    a 0.1 m section at or below L / 4 (a purely transverse |t| would bend many of
+    these beams by several times their length).
+    """
+    rng = np.random.default_rng(seed)
+    L = rng.uniform(0.5, 2.0, n)
+    s = rng.uniform(0.0, 1.0, n)
+    E = rng.uniform(1e3, 1e6, n)
+    nu = rng.uniform(0.3, 0.49, n)
+    tmag = rng.uniform(10.0, 1000.0, n)
+
+    def cells_for(p):
+        sp = s ** p
+        nx = np.rint(8 + 112 * sp).astype(np.int64)
+        ny = np.rint(2 + 8 * sp).astype(np.int64)
+        return nx, ny
+
+    lo, hi = 0.05, 20.0  # total tets decreases as p grows
+    for _ in range(60):
+        p = np.sqrt(lo * hi)
+        nx, ny = cells_for(p)
+        tot = float(np.sum(6 * nx * ny * ny))
+        if tot > target_tets:
+            lo = p
+        else:
+            hi = p
+    nx, ny = cells_for(np.sqrt(lo * hi))
+    out = []
+    for i in range(n):
+        m = box_tet4(float(L[i]), section, section, int(nx[i]), int(ny[i]), int(ny[i]))
+        tz = min(0.5 * tmag[i], E[i] / (1600.0 * L[i] ** 2))
+        out.append(BeamCase(m, float(L[i]), float(E[i]), float(nu[i]), np.array([tmag[i], 0.0, -tz]),
+                            (int(nx[i]), int(ny[i]), int(ny[i]))))
+    return out

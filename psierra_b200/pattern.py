@@ -16,6 +16,12 @@ from psierra_b200 import _lib
 from psierra_b200._lib import check, lib, ptr
 
 
+def torch_from(a: np.ndarray, device):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+
 class MeshPattern:
     def __init__(self, elements: np.ndarray, n_nodes: int):
         conn = np.ascontiguousarray(elements, dtype=np.int64)
@@ -48,6 +54,7 @@ class MeshPattern:
         self._blocks: tuple | None = None
         self._plan_host: dict | None = None
         self.granule, self.tile, self.tile_items, self.lag = self.QUEUE[npe]
+        self.blocks_per_sm = 0
 
     @property
     def n_dofs(self) -> int:
@@ -125,21 +132,46 @@ class MeshPattern:
                 setattr(st, k, d[k].data_ptr())
             st.pair_gptr = h["pair_gptr"].ctypes.data
             st.node_gptr = h["node_gptr"].ctypes.data
-            st.tile, st.lag, st.tile_items = self.tile, self.lag, self.tile_items
-            L = lib()
-            for key, with_pairs in (("k", 1), ("f", 0)):
-                nt = ctypes.c_int64()
-                check(L.psx_task_count(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag,
-                                       ctypes.byref(nt)), "psx_task_count")
-                tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
-                btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
-                check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag, ptr(tasks),
-                                      ptr(btiles)),
-                      "psx_task_fill")
-                d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
-                setattr(st, "n_tasks_" + key, int(nt.value))
-                setattr(st, "tasks_" + key, d["tasks_" + key].data_ptr())
-                setattr(st, "btiles_" + key, d["btiles_" + key].data_ptr())
             d["plan"] = st
+            self._build_tasks(d)
             self._dev = d
         return self._dev
+
+    def _build_tasks(self, d: dict) -> None:
+        """(Re)build the element/gather task queues of the plan in ``d`` for the current lag."""
+        t = lambda a: torch_from(a, d["device"])  # noqa: E731
+        st = d["plan"]
+        h = self.plan_host()
+        st.tile, st.lag, st.tile_items = self.tile, self.lag, self.tile_items
+        st.blocks_per_sm = self.blocks_per_sm
+        L = lib()
+        for key, with_pairs in (("k", 1), ("f", 0)):
+            nt = ctypes.c_int64()
+            check(L.psx_task_count(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag,
+                                   ctypes.byref(nt)), "psx_task_count")
+            tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
+            btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
+            check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag, ptr(tasks),
+                                  ptr(btiles)), "psx_task_fill")
+            d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
+            setattr(st, "n_tasks_" + key, int(nt.value))
+            setattr(st, "tasks_" + key, d["tasks_" + key].data_ptr())
+            setattr(st, "btiles_" + key, d["btiles_" + key].data_ptr())
+
+    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None) -> None:
+        """Change the persistent launch's lag (granules) and blocks per SM (0 = default).
+
+        Rebuilds the task queues when the lag changes; a workspace sized for the old lag
+        must be re-queried (``psx_work_bytes``) afterwards.
+        """
+        rebuild = lag is not None and int(lag) != self.lag
+        if lag is not None:
+            if int(lag) < 0:
+                raise ValueError("lag must be >= 0")
+            self.lag = int(lag)
+        if blocks_per_sm is not None:
+            self.blocks_per_sm = int(blocks_per_sm)
+        if self._dev is not None:
+            if rebuild:
+                self._build_tasks(self._dev)
+            self._dev["plan"].blocks_per_sm = self.blocks_per_sm

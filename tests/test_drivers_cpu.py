@@ -82,3 +82,22 @@ def test_line_search_rules():
         ls.search(lambda a: (_ for _ in ()).throw(KeyError("x")), 1.0, 1e-9)
     assert is_element_inversion_error(ValueError("Element inversion detected: det(F) = 0 <= 0."))
     assert not is_element_inversion_error(ValueError("something else"))
+
+
+def test_concat_meshes_offsets_and_beam_batch_ranges():
+    from psierra_b200 import meshgen
+
+    ms = [meshgen.box_tet4(1.0, 0.1, 0.1, n, 1, 1) for n in (2, 5, 3)]
+    u, no, eo = meshgen.concat_meshes(ms)
+    assert list(no) == [0, 12, 36, 52] and list(eo) == [0, 12, 42, 60]
+    assert np.array_equal(u.elements[12:42], ms[1].elements + 12)
+    assert np.array_equal(u.nodes[36:52], ms[2].nodes)
+    b = meshgen.beam_batch(n=32, target_tets=2e5, seed=1)
+    tot = sum(c.mesh.n_elements for c in b)
+    assert abs(tot - 2e5) < 0.05 * 2e5
+    for c in b:
+        nx, ny, nz = c.cells
+        assert 8 <= nx <= 120 and 2 <= ny <= 10 and ny == nz
+        assert 0.5 <= c.length <= 2.0 and 1e3 <= c.youngs <= 1e6 and 0.3 <= c.poisson <= 0.49
+        assert 10.0 <= c.traction[0] <= 1000.0 and c.traction[2] <= 0.0
+        assert 400.0 * -c.traction[2] * c.length ** 2 / c.youngs <= 0.25 + 1e-12
