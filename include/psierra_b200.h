@@ -144,6 +144,8 @@ typedef struct psx_plan {
   const int32_t* tasks_f;   /* device */
   const int32_t* btiles_k;  /* device, n_granules: gather tiles per granule in tasks_k */
   const int32_t* btiles_f;  /* device, n_granules: gather tiles per granule in tasks_f */
+  int32_t ring_slack;       /* ring granules beyond span + lag (>= 6; 0 = 6): room for tiles in flight */
+  int32_t lag_f;            /* lag of tasks_f (0 = lag); `lag` is the lag of tasks_k */
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */

@@ -98,6 +98,8 @@ class PlanStruct(ctypes.Structure):
         ("tasks_f", ctypes.c_void_p),
         ("btiles_k", ctypes.c_void_p),
         ("btiles_f", ctypes.c_void_p),
+        ("ring_slack", ctypes.c_int32),
+        ("lag_f", ctypes.c_int32),
     ]
 
 

@@ -94,12 +94,14 @@ class GPUAssembler:
         """Kernel launches one assemble() call makes (one persistent kernel)."""
         return 1
 
-    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None) -> None:
+    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None,
+                  ring_slack: int | None = None, lag_f: int | None = None) -> None:
         """Launch shape of the persistent kernel (see ``MeshPattern.set_queue``)."""
-        old = self.pattern.lag
-        self.pattern.set_queue(lag=lag, blocks_per_sm=blocks_per_sm)
-        if self.pattern.lag != old:
-            self._work.clear()  # the record ring is sized by the lag
+        p = self.pattern
+        old = (p.lag, p.lag_f, p.ring_slack)
+        p.set_queue(lag=lag, blocks_per_sm=blocks_per_sm, ring_slack=ring_slack, lag_f=lag_f)
+        if (p.lag, p.lag_f, p.ring_slack) != old:
+            self._work.clear()  # the record ring is sized by the lag and the slack
 
     def workspace(self, precision: str) -> torch.Tensor:
         w = self._work.get(precision)

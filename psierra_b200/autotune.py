@@ -1,10 +1,12 @@
 """Launch-shape autotuner of the persistent assembly kernel.
 
-Two knobs change the speed of ``psx_tet4_assemble`` / ``psx_tet10_assemble`` on a given
+Three knobs change the speed of ``psx_tet4_assemble`` / ``psx_tet10_assemble`` on a given
 mesh without changing a single output bit (each K and f entry is summed by one owner in
-a fixed order whatever the schedule): the lag (granules between an element tile and the
-gathers it completes, which trades L2-resident ring size for fewer waits) and the number
-of persistent blocks per SM.  ``tune`` times each candidate with CUDA events on the
+a fixed order whatever the schedule): the lag of the task queue in use (granules between
+an element tile and the gathers it completes: too small and gathers wait for elements
+still in flight, too large and the ring outgrows L2), the ring slack (room for element
+tiles in flight before they must wait for old gathers) and the number of persistent
+blocks per SM.  ``tune`` times each candidate with CUDA events on the
 caller's stream and keeps the fastest; results are cached per device, element type,
 mesh size and precision, in memory and optionally in a JSON file.
 """
@@ -15,10 +17,11 @@ import os
 
 import torch
 
-DEFAULT_LAGS = (4, 8, 16)
-DEFAULT_BLOCKS = (1, 2, 3)
+DEFAULT_LAGS = (8, 12, 16, 24)
+DEFAULT_BLOCKS = (2,)
+DEFAULT_SLACKS = (6, 12, 20)
 
-_cache: dict[str, tuple[int, int]] = {}
+_cache: dict[str, tuple[int, int, int]] = {}
 
 
 def _key(asm, precision: str, want_f: bool, want_k: bool) -> str:
@@ -39,12 +42,21 @@ def _time(asm, u, precision, want_f, want_k, f, k, reps: int) -> float:
     return a.elapsed_time(b) / reps
 
 
-def tune(asm, u: torch.Tensor, precision: str | None = None, want_f: bool = True, want_k: bool = True,
-         lags=DEFAULT_LAGS, blocks=DEFAULT_BLOCKS, reps: int = 5, cache_file: str | None = None) -> dict:
-    """Pick (lag, blocks_per_sm) for ``asm`` by timing; applies and returns the choice.
+def _apply(asm, want_k: bool, lag: int, bps: int, slack: int) -> None:
+    if want_k:
+        asm.set_queue(lag=lag, blocks_per_sm=bps, ring_slack=slack)
+    else:
+        asm.set_queue(lag_f=lag, blocks_per_sm=bps, ring_slack=slack)
 
-    Returns ``{"lag", "blocks_per_sm", "ms", "table": {(lag, bps): ms}}``.  With a cached
-    entry for the same key nothing is timed.
+
+def tune(asm, u: torch.Tensor, precision: str | None = None, want_f: bool = True, want_k: bool = True,
+         lags=DEFAULT_LAGS, blocks=DEFAULT_BLOCKS, slacks=DEFAULT_SLACKS, reps: int = 5,
+         cache_file: str | None = None) -> dict:
+    """Pick (lag, blocks_per_sm, ring_slack) for ``asm`` by timing; applies and returns it.
+
+    The lag tuned is that of the queue the sweep uses (the K queue when ``want_k``, else
+    the f queue).  Returns ``{"lag", "blocks_per_sm", "ring_slack", "ms", "table":
+    {(lag, bps, slack): ms}}``.  With a cached entry for the same key nothing is timed.
     """
     prec = precision or asm.precision
     key = _key(asm, prec, want_f, want_k)
@@ -54,20 +66,21 @@ def tune(asm, u: torch.Tensor, precision: str | None = None, want_f: bool = True
             disk = json.load(fh)
     hit = _cache.get(key) or (tuple(disk[key]) if key in disk else None)
     if hit is not None:
-        asm.set_queue(lag=hit[0], blocks_per_sm=hit[1])
-        return {"lag": hit[0], "blocks_per_sm": hit[1], "ms": None, "table": {}}
+        _apply(asm, want_k, *hit)
+        return {"lag": hit[0], "blocks_per_sm": hit[1], "ring_slack": hit[2], "ms": None, "table": {}}
     f = asm.new_f() if want_f else None
     k = asm.new_k(prec) if want_k else None
     table = {}
     for lag in lags:
         for bps in blocks:
-            asm.set_queue(lag=lag, blocks_per_sm=bps)
-            table[(lag, bps)] = _time(asm, u, prec, want_f, want_k, f, k, reps)
+            for slack in slacks:
+                _apply(asm, want_k, lag, bps, slack)
+                table[(lag, bps, slack)] = _time(asm, u, prec, want_f, want_k, f, k, reps)
     best = min(table, key=table.get)
-    asm.set_queue(lag=best[0], blocks_per_sm=best[1])
+    _apply(asm, want_k, *best)
     _cache[key] = best
     if cache_file:
         disk[key] = list(best)
         with open(cache_file, "w") as fh:
             json.dump(disk, fh, indent=1, sort_keys=True)
-    return {"lag": best[0], "blocks_per_sm": best[1], "ms": table[best], "table": table}
+    return {"lag": best[0], "blocks_per_sm": best[1], "ring_slack": best[2], "ms": table[best], "table": table}

@@ -367,11 +367,12 @@ inline int32_t device_sm_count() {
   return sms;
 }
 
-// Workspace of one assembly call: task counters, then the ring of K records, then the
-// ring of f records (each 256-byte aligned).  The ring spans a power-of-two number of
-// granules covering the item span plus the blocks in flight; with `work` null only the
-// sizes are computed.
-inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayout* W, int blocks_per_sm = 3) {
+// Workspace of one assembly call: task counters, then the ring of K records (the K queue
+// only), then the ring of f records (each 256-byte aligned).  The ring spans a
+// power-of-two number of granules covering the item span, the queue's lag and the
+// slack for tiles in flight; with `work` null only the sizes are computed.
+inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayout* W, int blocks_per_sm = 3,
+                       bool queue_k = true) {
   if (!P || !W || P->n_elements <= 0 || P->n_nodes <= 0 || P->granule <= 0 || (P->granule & (P->granule - 1)))
     return PSX_ERR_ARG;
   if (!P->conn || !P->pair_info || !P->pair_ptr || !P->pair_src || !P->node_info || !P->node_ptr ||
@@ -388,8 +389,12 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   W->span_g = (int32_t)((P->max_span + P->granule - 1) / P->granule);
   int32_t all = 1;
   while (all < P->n_granules) all <<= 1;
+  // element tiles overwrite ring slots only after the gathers reading them are done; the
+  // slack beyond span + lag is room for the element tiles in flight (at least 6 granules)
+  const int32_t slack = P->ring_slack > 6 ? P->ring_slack : 6;
   int32_t ring = 1;
-  while (ring < W->span_g + P->lag + 6) ring <<= 1;
+  const int32_t lag = queue_k || P->lag_f <= 0 ? P->lag : P->lag_f;
+  while (ring < W->span_g + lag + slack) ring <<= 1;
   W->ring_g = ring < all ? ring : all;
   W->ring_elems = (int64_t)W->ring_g * P->granule;
   const int sms = device_sm_count();
@@ -401,7 +406,7 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   W->grid = (int32_t)(sms * bps < ntask ? sms * bps : ntask);
   auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
   W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
-  const int64_t kbytes = up(W->ring_elems * kK * kt);
+  const int64_t kbytes = queue_k ? up(W->ring_elems * kK * kt) : 0;
   const int64_t fbytes = up(W->ring_elems * kF * 8);
   W->total_bytes = (int64_t)W->counter_bytes + kbytes + fbytes;
   W->counters = nullptr;

@@ -348,7 +348,7 @@ extern "C" int psx_tet10_assemble(const psx_plan_t* plan, const double* X, const
   if (wantF && !f_out) return PSX_ERR_ARG;
   if (wantK && !k_out) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, precision, work, &W, 2);
+  int rc = work_layout(plan, precision, work, &W, 2, wantK || linear);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet10Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};

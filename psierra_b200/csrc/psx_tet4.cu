@@ -34,6 +34,14 @@ constexpr int kModeAdjoint = 64;  // internal: vector-Jacobian product of f_int
 #define PSX_TET4_MIN_BLOCKS 2
 #endif
 constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the register budget targets
+// Register targets of the other instantiations (resident blocks per SM): the FP64 tangent,
+// and the sweeps that build no tangent (f only, K.v, dynamic relaxation, adjoint).
+#ifndef PSX_TET4_MIN_BLOCKS_K64
+#define PSX_TET4_MIN_BLOCKS_K64 2
+#endif
+#ifndef PSX_TET4_MIN_BLOCKS_NOK
+#define PSX_TET4_MIN_BLOCKS_NOK 2
+#endif
 
 struct Tet4Geom {
   double g[4][3];  // shape-function gradients
@@ -403,7 +411,14 @@ struct StageSmem {
 };
 
 template <typename KT, int MODE>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+constexpr int min_blocks() {
+  return (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) == 0 || (MODE & (PSX_KV | kModeAdjoint)) != 0
+             ? PSX_TET4_MIN_BLOCKS_NOK
+             : (sizeof(KT) == 4 ? kMinBlocks : PSX_TET4_MIN_BLOCKS_K64);
+}
+
+template <typename KT, int MODE>
+__global__ void __launch_bounds__(kThreads, min_blocks<KT, MODE>())
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
                        KT* __restrict__ k_out, double* __restrict__ f_out, DRArgs dr) {
   using L = RecLayout<4>;
@@ -485,8 +500,9 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   static unsigned long long s_smem_set = 0;
   if (smem > 0 && set_dynamic_smem_once(tet4_persistent_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess)
     return PSX_ERR_CUDA;
-  tet4_persistent_kernel<KT, MODE><<<W.grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
-                                                                      k_out, f_out, dr);
+  const int grid = W.grid;
+  tet4_persistent_kernel<KT, MODE><<<grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
+                                                                    k_out, f_out, dr);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }
@@ -497,12 +513,15 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
 extern "C" size_t psx_status_bytes(void) { return sizeof(psx::Status); }
 
 extern "C" int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t* ring_elems, int64_t* bytes) {
-  psx::WorkLayout W;
-  const int rc = psx::work_layout(plan, precision, nullptr, &W);
+  // one workspace serves both task queues: the larger of their layouts
+  psx::WorkLayout Wk, Wf;
+  int rc = psx::work_layout(plan, precision, nullptr, &Wk, 3, true);
+  if (rc != PSX_OK) return rc;
+  rc = psx::work_layout(plan, precision, nullptr, &Wf, 3, false);
   if (rc != PSX_OK) return rc;
   if (!ring_elems || !bytes) return PSX_ERR_ARG;
-  *ring_elems = W.ring_elems;
-  *bytes = W.total_bytes;
+  *ring_elems = Wk.ring_elems > Wf.ring_elems ? Wk.ring_elems : Wf.ring_elems;
+  *bytes = Wk.total_bytes > Wf.total_bytes ? Wk.total_bytes : Wf.total_bytes;
   return PSX_OK;
 }
 
@@ -520,7 +539,7 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   if (wantF && !f_out) return PSX_ERR_ARG;
   if (wantK && !k_out) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks, wantK || linear);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, nullptr, nullptr, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
@@ -541,7 +560,7 @@ extern "C" int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double
   using namespace psx;
   if (!plan || plan->npe != 4 || !X || !u || !v || !y_out || !status || !work) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks, false);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, v, nullptr, nullptr, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
@@ -557,7 +576,7 @@ extern "C" int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const d
   using namespace psx;
   if (!plan || plan->npe != 4 || !X || !u || !b || !minv || !x || !vel || !status || !work) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, precision, work, &W, kMinBlocks);
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks, false);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, x, nullptr, nullptr, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};
@@ -574,7 +593,7 @@ extern "C" int psx_tet4_adjoint(const psx_plan_t* plan, const double* X, const d
   using namespace psx;
   if (!plan || plan->npe != 4 || !X || !u || !w || !gX_out || !status || !work) return PSX_ERR_ARG;
   WorkLayout W;
-  int rc = work_layout(plan, PSX_FP64, work, &W, kMinBlocks);
+  int rc = work_layout(plan, PSX_FP64, work, &W, kMinBlocks, false);
   if (rc != PSX_OK) return rc;
   if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
   Tet4Args A{plan->conn, X, u, w, gmu_out, gkappa_out, mu_e, kappa_e, mu, kappa, 0.0, static_cast<Status*>(status)};

@@ -53,7 +53,7 @@ class MeshPattern:
         self._dev: dict | None = None
         self._blocks: tuple | None = None
         self._plan_host: dict | None = None
-        self.granule, self.tile, self.tile_items, self.lag = self.QUEUE[npe]
+        self.granule, self.tile, self.tile_items, self.lag, self.lag_f, self.ring_slack = self.QUEUE[npe]
         self.blocks_per_sm = 0
 
     @property
@@ -72,8 +72,11 @@ class MeshPattern:
             self._blocks = (blk_ptr, blk_src)
         return self._blocks
 
-    # queue geometry per element type: granule (elements), element tile, item tile, lag (granules)
-    QUEUE = {4: (4096, 32, 32, 8), 10: (512, 8, 32, 16)}
+    # queue geometry per element type: granule (elements), element tile, item tile, lag of
+    # the K queue, lag of the f / K.v queue (granules), ring slack (granules; 0 = 6).  The
+    # Tet4 values are the fastest of a lag x slack sweep on the 3.07M-element cube
+    # (FP32-mixed f+K and f / K.v timed separately).
+    QUEUE = {4: (4096, 32, 32, 8, 16, 12), 10: (512, 8, 32, 16, 16, 0)}
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
@@ -142,36 +145,46 @@ class MeshPattern:
         t = lambda a: torch_from(a, d["device"])  # noqa: E731
         st = d["plan"]
         h = self.plan_host()
-        st.tile, st.lag, st.tile_items = self.tile, self.lag, self.tile_items
+        st.tile, st.lag, st.lag_f, st.tile_items = self.tile, self.lag, self.lag_f, self.tile_items
         st.blocks_per_sm = self.blocks_per_sm
+        st.ring_slack = self.ring_slack
         L = lib()
-        for key, with_pairs in (("k", 1), ("f", 0)):
+        for key, with_pairs, lag in (("k", 1, self.lag), ("f", 0, self.lag_f)):
             nt = ctypes.c_int64()
-            check(L.psx_task_count(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag,
+            check(L.psx_task_count(ctypes.byref(st), with_pairs, self.tile, self.tile_items, lag,
                                    ctypes.byref(nt)), "psx_task_count")
             tasks = np.zeros(4 * max(int(nt.value), 1), dtype=np.int32)
             btiles = np.zeros(max(h["n_granules"], 1), dtype=np.int32)
-            check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.tile, self.tile_items, self.lag, ptr(tasks),
+            check(L.psx_task_fill(ctypes.byref(st), with_pairs, self.tile, self.tile_items, lag, ptr(tasks),
                                   ptr(btiles)), "psx_task_fill")
             d["tasks_" + key], d["btiles_" + key] = t(tasks), t(btiles)
             setattr(st, "n_tasks_" + key, int(nt.value))
             setattr(st, "tasks_" + key, d["tasks_" + key].data_ptr())
             setattr(st, "btiles_" + key, d["btiles_" + key].data_ptr())
 
-    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None) -> None:
-        """Change the persistent launch's lag (granules) and blocks per SM (0 = default).
+    def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None,
+                  ring_slack: int | None = None, lag_f: int | None = None) -> None:
+        """Change the persistent launch's lags (granules; ``lag`` for the K queue, ``lag_f``
+        for the f / K.v queue), blocks per SM (0 = default) and ring slack (granules beyond
+        span + lag; 0 = the minimum, 6).
 
-        Rebuilds the task queues when the lag changes; a workspace sized for the old lag
+        Rebuilds the task queues when a lag changes; a workspace sized for the old values
         must be re-queried (``psx_work_bytes``) afterwards.
         """
-        rebuild = lag is not None and int(lag) != self.lag
-        if lag is not None:
-            if int(lag) < 0:
+        rebuild = (lag is not None and int(lag) != self.lag) or (lag_f is not None and int(lag_f) != self.lag_f)
+        for v in (lag, lag_f):
+            if v is not None and int(v) < 0:
                 raise ValueError("lag must be >= 0")
+        if lag is not None:
             self.lag = int(lag)
+        if lag_f is not None:
+            self.lag_f = int(lag_f)
         if blocks_per_sm is not None:
             self.blocks_per_sm = int(blocks_per_sm)
+        if ring_slack is not None:
+            self.ring_slack = int(ring_slack)
         if self._dev is not None:
             if rebuild:
                 self._build_tasks(self._dev)
             self._dev["plan"].blocks_per_sm = self.blocks_per_sm
+            self._dev["plan"].ring_slack = self.ring_slack
