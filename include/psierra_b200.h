@@ -146,6 +146,14 @@ typedef struct psx_plan {
   const int32_t* btiles_f;  /* device, n_granules: gather tiles per granule in tasks_f */
   int32_t ring_slack;       /* ring granules beyond span + lag (>= 6; 0 = 6): room for tiles in flight */
   int32_t lag_f;            /* lag of tasks_f (0 = lag); `lag` is the lag of tasks_k */
+  /* Tet4 tile records (psx_tile_plan_fill; required when npe == 4, device arrays) */
+  int32_t tile_cap_pairs;   /* most distinct node pairs in one element tile */
+  int32_t tile_cap_nodes;   /* most distinct nodes in one element tile */
+  const uint8_t* tile_meta; /* n_tiles x psx_tile_meta_stride(tile) bytes (psx_tile_plan_fill) */
+  const int32_t* pair_ptr_t; /* n_pairs + 1 */
+  const int32_t* pair_src_t; /* tile * 256 + local pair, ascending tile */
+  const int32_t* node_ptr_t; /* N + 1 */
+  const int32_t* node_src_t; /* tile * 128 + local node, ascending tile */
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */
@@ -162,6 +170,25 @@ int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int3
                   const int32_t* nbr, int64_t granule, int32_t* pair_info, int32_t* pair_ptr,
                   int32_t* pair_src, int32_t* pair_gptr, int32_t* node_info, int32_t* node_ptr,
                   int32_t* node_src, int32_t* node_gptr, int64_t* max_span);
+
+/*
+ * Tile plan of the Tet4 kernels (host; no counterpart in the reference, which has no
+ * element tiles): the element tile of one warp (tile consecutive elements, tile <= 32,
+ * a power of two; the plan's `tile`) sums the blocks its elements share in shared
+ * memory and writes one record per distinct pair / node.  Inputs: conn (E x 4), the
+ * element-code item lists of psx_plan_fill.  Outputs (host buffers, n_tiles =
+ * ceil(E / tile)): meta (n_tiles x psx_tile_meta_stride(tile) bytes; per tile: pair and
+ * node counts, offsets and codes, laid out as psx_pattern.cpp describes), pair_ptr_t
+ * (n_pairs + 1), pair_src_t (<= len pair_src), node_ptr_t (N + 1), node_src_t (<= len
+ * node_src), caps[2] = {most pairs, most nodes in a tile}.  Contributions keep
+ * ascending element order inside a tile and ascending tile order across tiles (a
+ * fixed, reproducible summation order).
+ */
+int64_t psx_tile_meta_stride(int32_t tile);
+int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32_t tile, const int32_t* pair_ptr,
+                       const int32_t* pair_src, int64_t n_pairs, const int32_t* node_ptr, const int32_t* node_src,
+                       int64_t N, uint8_t* meta, int32_t* pair_ptr_t, int32_t* pair_src_t, int32_t* node_ptr_t,
+                       int32_t* node_src_t, int32_t* caps);
 
 /*
  * Task queue of the persistent assembly kernel (host): for each granule g, the

@@ -64,6 +64,8 @@ SIGNATURES: dict[str, list] = {
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_pcg_enqueue": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_segment_sumsq": [_i64, _p, _p, _p, _p],
+    "psx_tile_plan_fill": [_p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p],
+    "psx_tile_meta_stride": [_i32],
 }
 
 
@@ -100,6 +102,13 @@ class PlanStruct(ctypes.Structure):
         ("btiles_f", ctypes.c_void_p),
         ("ring_slack", ctypes.c_int32),
         ("lag_f", ctypes.c_int32),
+        ("tile_cap_pairs", ctypes.c_int32),
+        ("tile_cap_nodes", ctypes.c_int32),
+        ("tile_meta", ctypes.c_void_p),
+        ("pair_ptr_t", ctypes.c_void_p),
+        ("pair_src_t", ctypes.c_void_p),
+        ("node_ptr_t", ctypes.c_void_p),
+        ("node_src_t", ctypes.c_void_p),
     ]
 
 
@@ -121,6 +130,7 @@ def lib() -> ctypes.CDLL:
             fn.restype = ctypes.c_int
         L.psx_status_bytes.argtypes = []
         L.psx_status_bytes.restype = ctypes.c_size_t
+        L.psx_tile_meta_stride.restype = ctypes.c_int64
         _lib = L
     return _lib
 

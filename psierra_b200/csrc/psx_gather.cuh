@@ -38,6 +38,21 @@ struct GatherArgs {
   int32_t p0, p1;            // pair item range of this launch
   int32_t n0, n1;            // node item range of this launch
   int64_t ring_mask;
+  // tile records (Tet4): lists name (tile, local pair / node); a tile's ring slot holds
+  // cap_p pair blocks (12 values), cap_n diagonal blocks (8 values) and cap_n f triples
+  const int32_t* pair_ptr_t;
+  const int32_t* pair_src_t;  // tile * 256 + local pair
+  const int32_t* node_ptr_t;
+  const int32_t* node_src_t;  // tile * 128 + local node
+  int64_t ring_tile_mask;
+  int32_t cap_p, cap_n;
+  int32_t tile_k;             // K values per tile record: 12 cap_p + 8 cap_n
+  // per-tile reduction lists (psx_tile_plan_fill): one block of meta_stride bytes per
+  // tile, fields at byte offsets off_p (pair offsets), off_n (node offsets), src_p (pair
+  // codes), src_n (node codes); byte 0 / 1 = pair / node count
+  const uint8_t* tile_meta;
+  int32_t meta_stride, off_p, off_n, src_p, src_n;
+  int32_t tile;
 };
 
 // 16-byte vector loads/stores of record blocks (L2-only loads: the ring is rewritten while
@@ -87,12 +102,14 @@ struct Batch {
 
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list
 // (ascending element) order; their loads are issued kBatch at a time.
-template <typename KT, int NPE>
+template <typename KT, int NPE, bool TILES = false>
 __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, const KT* __restrict__ krec,
                                             KT* __restrict__ k_out) {
   using L = RecLayout<NPE>;
   const int4 info = __ldg(reinterpret_cast<const int4*>(g.pair_info) + p);
-  const int32_t s0 = __ldg(g.pair_ptr + p), s1 = __ldg(g.pair_ptr + p + 1);
+  const int32_t* list = TILES ? g.pair_src_t : g.pair_src;
+  const int32_t* lptr = TILES ? g.pair_ptr_t : g.pair_ptr;
+  const int32_t s0 = __ldg(lptr + p), s1 = __ldg(lptr + p + 1);
   KT acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = (KT)0;
@@ -100,12 +117,17 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
-    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(g.pair_src + s + b) : -1;
+    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(list + s + b) : -1;
     KT v[kBatch][12];
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
-      if (src[b] >= 0)
-        load_block<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * L::kK + L::pair_off(src[b] & 63), v[b]);
+      if (src[b] >= 0) {
+        if constexpr (TILES)
+          load_block<KT, 12>(krec + ((int64_t)(src[b] >> 8) & g.ring_tile_mask) * g.tile_k + 12 * (src[b] & 255),
+                             v[b]);
+        else
+          load_block<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * L::kK + L::pair_off(src[b] & 63), v[b]);
+      }
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (src[b] >= 0) {
@@ -133,13 +155,15 @@ struct DRArgs {
 };
 
 // Node item: diagonal block and/or f (or, with DR, the fused pseudo-step on f = K x).
-template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false>
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false, bool TILES = false>
 __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, const KT* __restrict__ krec,
                                             const double* __restrict__ frec, KT* __restrict__ k_out,
                                             double* __restrict__ f_out, const DRArgs* dr = nullptr) {
   using L = RecLayout<NPE>;
   const int4 info = __ldg(reinterpret_cast<const int4*>(g.node_info) + n);
-  const int32_t s0 = __ldg(g.node_ptr + n), s1 = __ldg(g.node_ptr + n + 1);
+  const int32_t* list = TILES ? g.node_src_t : g.node_src;
+  const int32_t* lptr = TILES ? g.node_ptr_t : g.node_ptr;
+  const int32_t s0 = __ldg(lptr + n), s1 = __ldg(lptr + n + 1);
   KT acc[6];
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc[j] = (KT)0;
@@ -148,17 +172,27 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
-    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(g.node_src + s + b) : -1;
+    for (int b = 0; b < kBatch; ++b) src[b] = (s + b < s1) ? __ldg(list + s + b) : -1;
     KT v[kBatch][8];
     double fv[kBatch][3];
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (src[b] >= 0) {
-        const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;
-        const int a = src[b] & 15;
-        if constexpr (WANT_K) load_block<KT, 8>(krec + slot * L::kK + L::diag_off(a), v[b]);
+        const KT* kp;
+        const double* fp;
+        if constexpr (TILES) {
+          const int64_t slot = (int64_t)(src[b] >> 7) & g.ring_tile_mask;
+          const int ln = src[b] & 127;
+          kp = krec + slot * g.tile_k + 12 * g.cap_p + 8 * ln;
+          fp = frec + slot * 3 * g.cap_n + 3 * ln;
+        } else {
+          const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;
+          const int a = src[b] & 15;
+          kp = krec + slot * L::kK + L::diag_off(a);
+          fp = frec + slot * L::kF + 3 * a;
+        }
+        if constexpr (WANT_K) load_block<KT, 8>(kp, v[b]);
         if constexpr (WANT_F) {
-          const double* fp = frec + slot * L::kF + 3 * a;
           fv[b][0] = __ldcg(fp);
           fv[b][1] = __ldcg(fp + 1);
           fv[b][2] = __ldcg(fp + 2);
@@ -284,7 +318,7 @@ __device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first,
 // the ring slots they overwrite are done, run `element_tile(task)` and publish their
 // granule; gather tiles wait for the element granules they read and sum them.  Every
 // wait is on a task earlier in the queue (psx_task_fill), so the queue always drains.
-template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR, typename ElementTile>
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR, bool TILES, typename ElementTile>
 __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs& Q, Status* st,
                                             const KT* __restrict__ krec, const double* __restrict__ frec,
                                             KT* __restrict__ k_out, double* __restrict__ f_out, const DRArgs& dr,
@@ -322,9 +356,9 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
       __syncwarp();
       for (int32_t item = task.z + lane; item < task.w; item += 32) {
         if (task.x == 1) {
-          if constexpr (WANT_K) gather_pair<KT, NPE>(g, item, krec, k_out);
+          if constexpr (WANT_K) gather_pair<KT, NPE, TILES>(g, item, krec, k_out);
         } else {
-          gather_node<KT, NPE, WANT_K, WANT_F, DR>(g, item, krec, frec, k_out, f_out, &dr);
+          gather_node<KT, NPE, WANT_K, WANT_F, DR, TILES>(g, item, krec, frec, k_out, f_out, &dr);
         }
       }
       __syncwarp();
@@ -343,6 +377,25 @@ inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
   g.node_src = P->node_src;
   g.p0 = g.p1 = g.n0 = g.n1 = 0;
   g.ring_mask = ring_elems - 1;
+  g.pair_ptr_t = P->pair_ptr_t;
+  g.pair_src_t = P->pair_src_t;
+  g.node_ptr_t = P->node_ptr_t;
+  g.node_src_t = P->node_src_t;
+  g.cap_p = P->tile_cap_pairs;
+  g.cap_n = P->tile_cap_nodes;
+  g.tile_k = 12 * g.cap_p + 8 * g.cap_n;
+  g.tile_meta = P->tile_meta;
+  g.tile = P->tile;
+  {
+    const int32_t T = P->tile > 0 ? P->tile : 1;
+    auto up4 = [](int32_t b) { return (b + 3) / 4 * 4; };
+    g.off_p = 4;
+    g.off_n = g.off_p + up4(6 * T + 1);
+    g.src_p = g.off_n + up4(4 * T + 1);
+    g.src_n = g.src_p + 6 * T;
+    g.meta_stride = (g.src_n + 4 * T + 15) / 16 * 16;
+  }
+  g.ring_tile_mask = P->tile > 0 ? ring_elems / P->tile - 1 : 0;
   return g;
 }
 
@@ -358,6 +411,7 @@ struct WorkLayout {
   int32_t granule_log2;
   int32_t grid;
   int64_t total_bytes;
+  bool tiles;  // tile records (Tet4, FP32 tangent or no tangent)
 };
 
 inline int32_t device_sm_count() {
@@ -380,6 +434,15 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
     return PSX_ERR_ARG;
   if (precision != PSX_FP64 && precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
   if (P->npe != 4 && P->npe != 10) return PSX_ERR_ARG;
+  // Tet4 sweeps with an FP32 tangent or without a tangent sum shared blocks per element
+  // tile (tile records); the FP64 tangent and Tet10 keep one record per element
+  W->tiles = P->npe == 4 && (precision == PSX_FP32_MIXED || !queue_k);
+  if (W->tiles) {
+    if (!P->tile_meta || !P->pair_ptr_t || !P->pair_src_t || !P->node_ptr_t || !P->node_src_t || P->tile_cap_nodes <= 0 ||
+        P->tile_cap_pairs < 0 || P->tile_cap_pairs > 192 || P->tile_cap_nodes > 128 || P->tile > 32 ||
+        (P->tile & (P->tile - 1)) || P->granule % P->tile)
+      return PSX_ERR_ARG;
+  }
   const int kt = precision == PSX_FP64 ? 8 : 4;
   const int kK = P->npe == 4 ? RecLayout<4>::kK : RecLayout<10>::kK;
   const int kF = P->npe == 4 ? RecLayout<4>::kF : RecLayout<10>::kF;
@@ -406,8 +469,15 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   W->grid = (int32_t)(sms * bps < ntask ? sms * bps : ntask);
   auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
   W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
-  const int64_t kbytes = queue_k ? up(W->ring_elems * kK * kt) : 0;
-  const int64_t fbytes = up(W->ring_elems * kF * 8);
+  int64_t kbytes, fbytes;
+  if (W->tiles) {
+    const int64_t ring_tiles = W->ring_elems / P->tile;
+    kbytes = queue_k ? up(ring_tiles * (12 * (int64_t)P->tile_cap_pairs + 8 * (int64_t)P->tile_cap_nodes) * kt) : 0;
+    fbytes = up(ring_tiles * 3 * (int64_t)P->tile_cap_nodes * 8);
+  } else {
+    kbytes = queue_k ? up(W->ring_elems * kK * kt) : 0;
+    fbytes = up(W->ring_elems * kF * 8);
+  }
   W->total_bytes = (int64_t)W->counter_bytes + kbytes + fbytes;
   W->counters = nullptr;
   W->krec = nullptr;

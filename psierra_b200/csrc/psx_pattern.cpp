@@ -322,6 +322,128 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
 }
 
 // ---------------------------------------------------------------------------
+// Tile plan (Tet4): the element tile of one warp (T consecutive elements) sums the
+// blocks its elements share before anything leaves the SM.  Per tile, the distinct
+// node pairs (and nodes) get local indices in order of first occurrence; for each
+// local pair the tile lists its contributions (element-in-tile * 8 + slot) in element
+// order.  Everything one tile needs is one contiguous block (psx_tile_meta_stride
+// bytes, a multiple of 16) so that a warp copies it to shared memory in one go:
+//   [0] np  [1] nn  [2..3] 0
+//   pair offsets  (np + 1 bytes, in a 4-byte-rounded field of 6T + 1)
+//   node offsets  (nn + 1 bytes, in a 4-byte-rounded field of 4T + 1)
+//   pair codes    (6T bytes, by local pair, element order within a pair)
+//   node codes    (4T bytes, element-in-tile * 4 + local node)
+// The gather lists then name (tile, local index) records instead of element slots, and
+// consecutive contributions of one tile collapse into one.
+namespace {
+inline int64_t up4(int64_t b) { return (b + 3) / 4 * 4; }
+struct TileMeta {
+  int64_t off_p, off_n, src_p, src_n, stride;
+  explicit TileMeta(int64_t T) {
+    off_p = 4;
+    off_n = off_p + up4(6 * T + 1);
+    src_p = off_n + up4(4 * T + 1);
+    src_n = src_p + 6 * T;
+    stride = (src_n + 4 * T + 15) / 16 * 16;
+  }
+};
+}  // namespace
+
+extern "C" int64_t psx_tile_meta_stride(int32_t T) { return T > 0 ? TileMeta(T).stride : 0; }
+
+extern "C" int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32_t T, const int32_t* pair_ptr,
+                                  const int32_t* pair_src, int64_t n_pairs, const int32_t* node_ptr,
+                                  const int32_t* node_src, int64_t N, uint8_t* meta, int32_t* pair_ptr_t,
+                                  int32_t* pair_src_t, int32_t* node_ptr_t, int32_t* node_src_t, int32_t* caps) {
+  if (!args_ok(conn, E, npe, N) || npe != 4 || T <= 0 || T > 32 || (T & (T - 1)) || !pair_ptr || !pair_src ||
+      !node_ptr || !node_src || !meta || !pair_ptr_t || !pair_src_t || !node_ptr_t || !node_src_t || !caps ||
+      n_pairs < 0)
+    return PSX_ERR_ARG;
+  constexpr int kP = 6;  // local pairs of a Tet4
+  const int64_t n_tiles = (E + T - 1) / T;
+  if (n_tiles >= ((int64_t)1 << 23)) return PSX_ERR_LIMIT;  // codes t * 256 + lp must fit int32
+  const TileMeta M(T);
+  static const int pa[kP] = {0, 0, 0, 1, 1, 2}, pb[kP] = {1, 2, 3, 2, 3, 3};  // local_pair_index order
+  std::vector<uint8_t> slot_lp((size_t)E * kP), node_ln((size_t)E * 4);
+  std::vector<std::pair<int64_t, int32_t>> keys;
+  keys.reserve(kP * T);
+  std::vector<std::pair<int32_t, int32_t>> first;
+  int32_t cap_p = 0, cap_n = 0;
+  std::memset(meta, 0, (size_t)(n_tiles * M.stride));
+  // Group (key, code) entries of one tile: local indices in order of first occurrence,
+  // each group's codes ascending.  Writes codes to src and offsets to off.
+  auto group = [&](uint8_t* src, uint8_t* off, std::vector<uint8_t>& map, int64_t e0, int per,
+                   int shift) -> int32_t {
+    std::sort(keys.begin(), keys.end());  // by key, then code
+    first.clear();                         // (first code, start in keys)
+    for (size_t k = 0; k < keys.size(); ++k)
+      if (k == 0 || keys[k].first != keys[k - 1].first) first.push_back({keys[k].second, (int32_t)k});
+    std::sort(first.begin(), first.end());
+    int32_t pos = 0, local = 0;
+    for (const auto& f : first) {
+      off[local] = (uint8_t)pos;
+      for (size_t k = f.second; k < keys.size() && keys[k].first == keys[f.second].first; ++k) {
+        const int32_t code = keys[k].second;
+        src[pos++] = (uint8_t)code;
+        map[(size_t)(e0 + (code >> shift)) * per + (code & ((1 << shift) - 1))] = (uint8_t)local;
+      }
+      ++local;
+    }
+    off[local] = (uint8_t)pos;
+    return local;
+  };
+  for (int64_t t = 0; t < n_tiles; ++t) {
+    const int64_t e0 = t * T, e1 = std::min<int64_t>(E, e0 + T);
+    uint8_t* m = meta + t * M.stride;
+    keys.clear();
+    for (int64_t e = e0; e < e1; ++e)
+      for (int s = 0; s < kP; ++s) {
+        const int64_t i = conn[e * 4 + pa[s]], j = conn[e * 4 + pb[s]];
+        keys.push_back({std::min(i, j) * N + std::max(i, j), (int32_t)((e - e0) * 8 + s)});
+      }
+    const int32_t np = group(m + M.src_p, m + M.off_p, slot_lp, e0, kP, 3);
+    keys.clear();
+    for (int64_t e = e0; e < e1; ++e)
+      for (int a = 0; a < 4; ++a) keys.push_back({conn[e * 4 + a], (int32_t)((e - e0) * 4 + a)});
+    const int32_t nn = group(m + M.src_n, m + M.off_n, node_ln, e0, 4, 2);
+    m[0] = (uint8_t)np;
+    m[1] = (uint8_t)nn;
+    cap_p = std::max(cap_p, np);
+    cap_n = std::max(cap_n, nn);
+  }
+  int32_t lg = 0;
+  while ((1 << lg) < T) ++lg;
+  // gather lists: element codes -> (tile, local) codes, consecutive duplicates merged
+  int64_t out = 0;
+  pair_ptr_t[0] = 0;
+  for (int64_t k = 0; k < n_pairs; ++k) {
+    int64_t last = -1;
+    for (int32_t q = pair_ptr[k]; q < pair_ptr[k + 1]; ++q) {
+      const int64_t e = pair_src[q] >> 6, slot = pair_src[q] & 63;
+      const int64_t c = (e >> lg) * 256 + slot_lp[(size_t)e * kP + slot];
+      if (c != last) pair_src_t[out++] = (int32_t)c;
+      last = c;
+    }
+    pair_ptr_t[k + 1] = (int32_t)out;
+  }
+  out = 0;
+  node_ptr_t[0] = 0;
+  for (int64_t k = 0; k < N; ++k) {
+    int64_t last = -1;
+    for (int32_t q = node_ptr[k]; q < node_ptr[k + 1]; ++q) {
+      const int64_t e = node_src[q] >> 4, a = node_src[q] & 15;
+      const int64_t c = (e >> lg) * 128 + node_ln[(size_t)e * 4 + a];
+      if (c != last) node_src_t[out++] = (int32_t)c;
+      last = c;
+    }
+    node_ptr_t[k + 1] = (int32_t)out;
+  }
+  caps[0] = cap_p;
+  caps[1] = cap_n;
+  return PSX_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Task queue of the persistent assembly kernel: for each granule g, the element
 // tiles of g followed by the gather tiles made ready by granule g-1-lag (pairs, then
 // nodes); the gather tiles of the last granules close the queue.  The lag keeps gather

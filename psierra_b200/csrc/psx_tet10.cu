@@ -270,7 +270,7 @@ tet10_persistent_kernel(Tet10Args A, GatherArgs g, QueueArgs Q, KT* __restrict__
   extern __shared__ __align__(16) unsigned char s_raw[];
   Tet10Smem<KT>& sm = reinterpret_cast<Tet10Smem<KT>*>(s_raw)[threadIdx.x >> 5];
   auto element_tile = [&](const int4& task) { tet10_tile<KT, MODE>(A, task, g.ring_mask, krec, frec, sm); };
-  drain_queue<KT, 10, kWantK, kWantF, false>(g, Q, A.st, krec, frec, k_out, f_out, DRArgs{}, element_tile);
+  drain_queue<KT, 10, kWantK, kWantF, false, false>(g, Q, A.st, krec, frec, k_out, f_out, DRArgs{}, element_tile);
 }
 
 // det J and det F at the 4 quadrature points of one element (error messages).

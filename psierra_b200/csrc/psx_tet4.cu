@@ -109,7 +109,21 @@ struct Tet4Args {
 // PSX_LINEAR, tet4_base.py:129-136) in the closed form of psx_common.cuh.
 // `krec` is global memory when KGLOBAL, else the shared-memory staging slot of the lane;
 // `frec` is always global memory.
-template <typename KT, int MODE, bool KGLOBAL = true>
+// 12 f / y doubles of an element: an L2-only store to the global ring, or plain stores to
+// the shared-memory staging of the element tile.
+template <bool FGLOBAL>
+__device__ __forceinline__ void store_f12(double* __restrict__ frec, const double v[12]) {
+  if constexpr (FGLOBAL) {
+    double2* fq = reinterpret_cast<double2*>(frec);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(v[2 * i], v[2 * i + 1]));
+  } else {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) frec[i] = v[i];
+  }
+}
+
+template <typename KT, int MODE, bool KGLOBAL = true, bool FGLOBAL = true>
 __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
                                              double* __restrict__ frec) {
   using L = RecLayout<4>;
@@ -187,9 +201,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 #pragma unroll
         for (int i = 0; i < 3; ++i)
           fr[3 * a + i] = G.V * (ps.P[i][0] * G.g[a][0] + ps.P[i][1] * G.g[a][1] + ps.P[i][2] * G.g[a][2]);
-      double2* fq = reinterpret_cast<double2*>(frec);
-#pragma unroll
-      for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(fr[2 * i], fr[2 * i + 1]));
+      store_f12<FGLOBAL>(frec, fr);
     }
     if constexpr (kWantK || kKV) {
       tc = tangent_coef<KT>(ps, kappa, G.V);
@@ -354,9 +366,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
         if (A.dkappa) A.dkappa[e] = G.V * ps_lnJ * FTL;
       }
     }
-    double2* fq = reinterpret_cast<double2*>(frec);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(yr[2 * i], yr[2 * i + 1]));
+    store_f12<FGLOBAL>(frec, yr);
   }
   if constexpr (kWantK) {
     // K_ab[k][m] = p_a,k w_b,m + p_b,k h_a,m + y_a,k p_b,m + s_ab d_km
@@ -400,15 +410,111 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 // tiles still reading the ring slots they overwrite are done.  Every wait is on tasks
 // that earlier warps have already claimed, so the queue always drains.  There are no
 // block-wide barriers: warps of a block progress independently.
-// Records of a warp's 32 consecutive elements are staged in shared memory (FP32) and
-// copied to the ring as one contiguous block, so the ring sees whole-sector writes.
-constexpr int kStageStride = RecLayout<4>::kK + 4;  // floats per staged record (bank spread)
+//
+// Tile records (FP32 tangent, and every sweep without a tangent): the 32 elements of a
+// warp's tile stage their blocks and f triples in shared memory; the warp then sums the
+// blocks its elements share (psx_tile_plan_fill: local pairs / nodes in first-occurrence
+// order, contributions in element order) and writes one record per distinct pair and
+// node, with consecutive lanes on consecutive records.  The FP64 tangent writes one
+// record per element straight to the ring.
+constexpr int kStageStride = RecLayout<4>::kK + 4;  // floats per staged element record (bank spread)
 
-template <typename KT>
-struct StageSmem {
-  static constexpr bool kOn = sizeof(KT) == 4;
-  static constexpr int kWarpFloats = kOn ? 32 * kStageStride : 1;
+// Largest per-tile meta block the shared-memory list area holds (tile = 32).
+constexpr int kMetaBytes = 656;
+
+template <typename KT, int MODE>
+struct Tet4Smem {
+  static constexpr bool kKV = (MODE & (PSX_KV | kModeAdjoint)) != 0;
+  static constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && !kKV;
+  static constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
+  static constexpr bool kTiles = sizeof(KT) == 4 || !kWantK;
+  static constexpr int kKFloats = kTiles && kWantK ? 32 * kStageStride : 0;  // per warp
+  static constexpr int kFDoubles = kTiles && kWantF ? 32 * 12 : 0;          // per warp
+  static constexpr int kMeta = kTiles ? kMetaBytes : 0;                       // per warp
+  static constexpr size_t kWarpBytes = sizeof(float) * kKFloats + sizeof(double) * kFDoubles + kMeta;
 };
+
+// Asynchronous 16-byte global -> shared copies (no registers held while in flight).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Start copying tile t's meta block into the warp's list area.
+__device__ __forceinline__ void tile_meta_prefetch(const GatherArgs& g, int64_t t, unsigned char* lst) {
+  const int lane = threadIdx.x & 31;
+  const uint4* src = reinterpret_cast<const uint4*>(g.tile_meta + t * g.meta_stride);
+  for (int c = lane; c < g.meta_stride / 16; c += 32) cp_async16(lst + 16 * c, src + c);
+}
+
+// Sum the staged element blocks of tile `t` into its tile record (one warp), with the
+// tile's lists in shared memory (`lst`, tile_meta_prefetch).
+template <bool WANT_K, bool WANT_F>
+__device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, const unsigned char* __restrict__ lst,
+                                            const float* __restrict__ kst, const double* __restrict__ fst,
+                                            float* __restrict__ krec, double* __restrict__ frec) {
+  using L = RecLayout<4>;
+  const int lane = threadIdx.x & 31;
+  const int64_t slot = t & g.ring_tile_mask;
+  if constexpr (WANT_K) {
+    const int np = lst[0];
+    const unsigned char* off = lst + g.off_p;
+    const unsigned char* src = lst + g.src_p;
+    float4* rec = reinterpret_cast<float4*>(krec + slot * g.tile_k);
+    for (int lp = lane; lp < np; lp += 32) {
+      const int a0 = off[lp], a1 = off[lp + 1];
+      float4 s[3] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                     make_float4(0.f, 0.f, 0.f, 0.f)};
+      for (int q = a0; q < a1; ++q) {
+        const int c = src[q];
+        const float4* b = reinterpret_cast<const float4*>(kst + (c >> 3) * kStageStride + L::pair_off(c & 7));
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const float4 x = b[r];
+          s[r].x += x.x; s[r].y += x.y; s[r].z += x.z; s[r].w += x.w;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) __stcg(rec + 3 * lp + r, s[r]);
+    }
+  }
+  const int nn = lst[1];
+  const unsigned char* off = lst + g.off_n;
+  const unsigned char* src = lst + g.src_n;
+  float4* drec = reinterpret_cast<float4*>(krec + slot * g.tile_k + 12 * g.cap_p);
+  double* frow = frec + slot * 3 * g.cap_n;
+  for (int ln = lane; ln < nn; ln += 32) {
+    const int a0 = off[ln], a1 = off[ln + 1];
+    float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f), d1 = d0;
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    for (int q = a0; q < a1; ++q) {
+      const int c = src[q];
+      const int el = c >> 2, a = c & 3;
+      if constexpr (WANT_K) {
+        const float4* b = reinterpret_cast<const float4*>(kst + el * kStageStride + L::diag_off(a));
+        const float4 x = b[0], y = b[1];
+        d0.x += x.x; d0.y += x.y; d0.z += x.z; d0.w += x.w;
+        d1.x += y.x; d1.y += y.y; d1.z += y.z; d1.w += y.w;
+      }
+      if constexpr (WANT_F) {
+        const double* fp = fst + el * 12 + 3 * a;
+        f0 += fp[0];
+        f1 += fp[1];
+        f2 += fp[2];
+      }
+    }
+    if constexpr (WANT_K) {
+      __stcg(drec + 2 * ln, d0);
+      __stcg(drec + 2 * ln + 1, d1);
+    }
+    if constexpr (WANT_F) {
+      __stcg(frow + 3 * ln, f0);
+      __stcg(frow + 3 * ln + 1, f1);
+      __stcg(frow + 3 * ln + 2, f2);
+    }
+  }
+}
 
 template <typename KT, int MODE>
 constexpr int min_blocks() {
@@ -422,30 +528,27 @@ __global__ void __launch_bounds__(kThreads, min_blocks<KT, MODE>())
 tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
                        KT* __restrict__ k_out, double* __restrict__ f_out, DRArgs dr) {
   using L = RecLayout<4>;
-  constexpr bool kKV = (MODE & (PSX_KV | kModeAdjoint)) != 0;
+  using S = Tet4Smem<KT, MODE>;
   constexpr bool kDR = (MODE & kModeDR) != 0;
-  constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && !kKV;
   const int lane = threadIdx.x & 31;
-  constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
-  extern __shared__ __align__(16) float s_stage[];  // kThreads/32 warps x kWarpFloats (FP32 K only)
-  float* my_stage = s_stage + (threadIdx.x >> 5) * StageSmem<KT>::kWarpFloats;
+  extern __shared__ __align__(16) unsigned char s_stage[];  // kThreads/32 warps x S::kWarpBytes
+  unsigned char* my_stage = s_stage + (threadIdx.x >> 5) * S::kWarpBytes;
+  float* kst = reinterpret_cast<float*>(my_stage);
+  double* fst = reinterpret_cast<double*>(my_stage + sizeof(float) * S::kKFloats);
+  unsigned char* lst = my_stage + sizeof(float) * S::kKFloats + sizeof(double) * S::kFDoubles;
   auto element_tile = [&](const int4& task) {
-    if constexpr (kStage) {
-      // tiles are 32 consecutive elements inside one granule: their ring slots are contiguous
+    if constexpr (S::kTiles) {
+      // a tile is `g.tile` consecutive elements starting at a multiple of g.tile; its
+      // lists arrive in shared memory while the elements are evaluated
+      const int64_t t = task.z / g.tile;
+      tile_meta_prefetch(g, t, lst);
       const int64_t e = task.z + (int64_t)lane;
-      const int64_t slot0 = (int64_t)task.z & g.ring_mask;
       if (e < task.w)
-        tet4_element<KT, MODE, false>(A, e, reinterpret_cast<KT*>(my_stage + lane * kStageStride),
-                                      frec + (e & g.ring_mask) * L::kF);
+        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride), fst + 12 * lane);
+      cp_async_wait_all();
       __syncwarp();
-      const int n = task.w - task.z;
-      float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(krec) + slot0 * L::kK);
-      constexpr int kChunks = L::kK / 4;  // float4 per record
-      for (int c = lane; c < n * kChunks; c += 32) {
-        const int el = c / kChunks, q = c - el * kChunks;
-        __stcg(dst + c, *reinterpret_cast<const float4*>(my_stage + el * kStageStride + 4 * q));
-      }
+      tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
+      __syncwarp();  // the staging and the lists are reused by the warp's next tile
     } else {
       for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
         const int64_t slot = e & g.ring_mask;
@@ -453,7 +556,7 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
       }
     }
   };
-  drain_queue<KT, 4, kWantK, kWantF, kDR>(g, Q, A.st, krec, frec, k_out, f_out, dr, element_tile);
+  drain_queue<KT, 4, S::kWantK, S::kWantF, kDR, S::kTiles>(g, Q, A.st, krec, frec, k_out, f_out, dr, element_tile);
 }
 
 __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
@@ -494,9 +597,13 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   Q.span_g = W.span_g;
   Q.ring_g = W.ring_g;
   Q.n_elements = P->n_elements;
+  using S = Tet4Smem<KT, MODE>;
+  // the kernel's record format (tile or element records) must be the one the workspace
+  // was laid out for
+  if (W.tiles != S::kTiles) return PSX_ERR_ARG;
+  if (S::kTiles && (P->tile > 32 || g.tile_k % 4 || g.meta_stride > kMetaBytes)) return PSX_ERR_ARG;
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
-  constexpr bool kStage = StageSmem<KT>::kOn && kWantK;
-  const size_t smem = kStage ? sizeof(float) * (kThreads / 32) * StageSmem<KT>::kWarpFloats : 0;
+  const size_t smem = (kThreads / 32) * S::kWarpBytes;
   static unsigned long long s_smem_set = 0;
   if (smem > 0 && set_dynamic_smem_once(tet4_persistent_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess)
     return PSX_ERR_CUDA;

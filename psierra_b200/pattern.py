@@ -105,8 +105,34 @@ class MeshPattern:
                                   ptr(h["node_info"]), ptr(h["node_ptr"]), ptr(h["node_src"]), ptr(h["node_gptr"]),
                                   ptr(h["max_span"])), "psx_plan_fill")
             h["n_pairs"], h["n_granules"] = P, ng
+            if npe == 4:
+                h.update(self._tile_plan(h, P))
             self._plan_host = h
         return self._plan_host
+
+    def _tile_plan(self, h: dict, n_pairs: int) -> dict:
+        """Tile records of the Tet4 kernels (``psx_tile_plan_fill``)."""
+        E, N, T = self.n_elements, self.n_nodes, self.tile
+        nt = (E + T - 1) // T
+        L = lib()
+        stride = int(L.psx_tile_meta_stride(T))
+        i32 = lambda n: np.zeros(max(int(n), 1), dtype=np.int32)  # noqa: E731
+        t = {
+            "tile_meta": np.zeros(nt * stride, dtype=np.uint8),
+            "pair_ptr_t": i32(n_pairs + 1), "pair_src_t": i32(h["pair_src"].size),
+            "node_ptr_t": i32(N + 1), "node_src_t": i32(h["node_src"].size),
+        }
+        caps = np.zeros(2, dtype=np.int32)
+        check(L.psx_tile_plan_fill(ptr(self.conn), E, 4, T, ptr(h["pair_ptr"]), ptr(h["pair_src"]), n_pairs,
+                                   ptr(h["node_ptr"]), ptr(h["node_src"]), N, ptr(t["tile_meta"]), ptr(t["pair_ptr_t"]),
+                                   ptr(t["pair_src_t"]), ptr(t["node_ptr_t"]), ptr(t["node_src_t"]), ptr(caps)),
+              "psx_tile_plan_fill")
+        # trim the upper-bound lists to what was written
+        t["pair_src_t"] = t["pair_src_t"][: max(int(t["pair_ptr_t"][-1]), 1)].copy()
+        t["node_src_t"] = t["node_src_t"][: max(int(t["node_ptr_t"][-1]), 1)].copy()
+        t["tile_caps"] = caps
+        t["tile_meta_stride"] = stride
+        return t
 
     def device(self, device) -> dict:
         """Device copies of the arrays the kernels read (uploaded once)."""
@@ -135,6 +161,11 @@ class MeshPattern:
                 setattr(st, k, d[k].data_ptr())
             st.pair_gptr = h["pair_gptr"].ctypes.data
             st.node_gptr = h["node_gptr"].ctypes.data
+            if self.npe == 4:
+                for k in ("tile_meta", "pair_ptr_t", "pair_src_t", "node_ptr_t", "node_src_t"):
+                    d[k] = t(h[k])
+                    setattr(st, k, d[k].data_ptr())
+                st.tile_cap_pairs, st.tile_cap_nodes = int(h["tile_caps"][0]), int(h["tile_caps"][1])
             d["plan"] = st
             self._build_tasks(d)
             self._dev = d
