@@ -80,7 +80,13 @@ __device__ __forceinline__ void load_block(const KT* __restrict__ p, KT v[N]) {
 // generic pointer (used for the shared-memory staging of records).
 template <typename KT, int N, bool GLOBAL = true>
 __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
-  if constexpr (!GLOBAL) {
+  if constexpr (!GLOBAL && sizeof(KT) == 4) {
+    // shared-memory staging: 16-byte stores (a record stride of 108 floats keeps the
+    // 8 lanes of each store phase on distinct banks)
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) q[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  } else if constexpr (!GLOBAL) {
 #pragma unroll
     for (int i = 0; i < N; ++i) p[i] = v[i];
   } else if constexpr (sizeof(KT) == 4) {

@@ -118,8 +118,9 @@ __device__ __forceinline__ void store_f12(double* __restrict__ frec, const doubl
 #pragma unroll
     for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(v[2 * i], v[2 * i + 1]));
   } else {
+    double2* fq = reinterpret_cast<double2*>(frec);
 #pragma unroll
-    for (int i = 0; i < 12; ++i) frec[i] = v[i];
+    for (int i = 0; i < 6; ++i) fq[i] = make_double2(v[2 * i], v[2 * i + 1]);
   }
 }
 
@@ -418,6 +419,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 // node, with consecutive lanes on consecutive records.  The FP64 tangent writes one
 // record per element straight to the ring.
 constexpr int kStageStride = RecLayout<4>::kK + 4;  // floats per staged element record (bank spread)
+constexpr int kFStride = 14;                        // doubles per staged f triple set (bank spread)
 
 // Largest per-tile meta block the shared-memory list area holds (tile = 32).
 constexpr int kMetaBytes = 656;
@@ -429,7 +431,7 @@ struct Tet4Smem {
   static constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 || kKV;
   static constexpr bool kTiles = sizeof(KT) == 4 || !kWantK;
   static constexpr int kKFloats = kTiles && kWantK ? 32 * kStageStride : 0;  // per warp
-  static constexpr int kFDoubles = kTiles && kWantF ? 32 * 12 : 0;          // per warp
+  static constexpr int kFDoubles = kTiles && kWantF ? 32 * kFStride : 0;    // per warp
   static constexpr int kMeta = kTiles ? kMetaBytes : 0;                       // per warp
   static constexpr size_t kWarpBytes = sizeof(float) * kKFloats + sizeof(double) * kFDoubles + kMeta;
 };
@@ -498,7 +500,7 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
         d1.x += y.x; d1.y += y.y; d1.z += y.z; d1.w += y.w;
       }
       if constexpr (WANT_F) {
-        const double* fp = fst + el * 12 + 3 * a;
+        const double* fp = fst + el * kFStride + 3 * a;
         f0 += fp[0];
         f1 += fp[1];
         f2 += fp[2];
@@ -544,7 +546,8 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
       tile_meta_prefetch(g, t, lst);
       const int64_t e = task.z + (int64_t)lane;
       if (e < task.w)
-        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride), fst + 12 * lane);
+        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
+                                             fst + kFStride * lane);
       cp_async_wait_all();
       __syncwarp();
       tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
