@@ -34,13 +34,22 @@ constexpr int kModeAdjoint = 64;  // internal: vector-Jacobian product of f_int
 #define PSX_TET4_MIN_BLOCKS 2
 #endif
 constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the register budget targets
-// Register targets of the other instantiations (resident blocks per SM): the FP64 tangent,
-// and the sweeps that build no tangent (f only, K.v, dynamic relaxation, adjoint).
+// Register targets of the other instantiations (resident blocks per SM, which is also
+// the default grid): the FP32 tangent without f, the FP64 tangent, the sweeps that build
+// no tangent (f only, K.v, dynamic relaxation) and the adjoint.  Chosen by timing the
+// 3.07M-element cube: more resident warps hide the element phase's latency, as long as
+// the element tile fits the budget without spilling.
+#ifndef PSX_TET4_MIN_BLOCKS_K32
+#define PSX_TET4_MIN_BLOCKS_K32 3
+#endif
 #ifndef PSX_TET4_MIN_BLOCKS_K64
 #define PSX_TET4_MIN_BLOCKS_K64 2
 #endif
 #ifndef PSX_TET4_MIN_BLOCKS_NOK
-#define PSX_TET4_MIN_BLOCKS_NOK 2
+#define PSX_TET4_MIN_BLOCKS_NOK 4
+#endif
+#ifndef PSX_TET4_MIN_BLOCKS_ADJ
+#define PSX_TET4_MIN_BLOCKS_ADJ 2
 #endif
 
 struct Tet4Geom {
@@ -520,9 +529,10 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
 
 template <typename KT, int MODE>
 constexpr int min_blocks() {
-  return (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) == 0 || (MODE & (PSX_KV | kModeAdjoint)) != 0
+  return (MODE & kModeAdjoint) != 0 ? PSX_TET4_MIN_BLOCKS_ADJ
+         : (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) == 0 || (MODE & PSX_KV) != 0
              ? PSX_TET4_MIN_BLOCKS_NOK
-             : (sizeof(KT) == 4 ? kMinBlocks : PSX_TET4_MIN_BLOCKS_K64);
+             : (sizeof(KT) == 8 ? PSX_TET4_MIN_BLOCKS_K64 : ((MODE & PSX_WANT_F) ? kMinBlocks : PSX_TET4_MIN_BLOCKS_K32));
 }
 
 template <typename KT, int MODE>
@@ -610,7 +620,14 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   static unsigned long long s_smem_set = 0;
   if (smem > 0 && set_dynamic_smem_once(tet4_persistent_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess)
     return PSX_ERR_CUDA;
-  const int grid = W.grid;
+  // one block per SM per register-target block, unless the plan overrides it
+  int grid = W.grid;
+  if (P->blocks_per_sm <= 0) {
+    const int64_t ntask = Q.n_tasks;
+    const int64_t want = (int64_t)device_sm_count() * min_blocks<KT, MODE>();
+    grid = (int)(want < ntask ? want : ntask);
+    if (grid <= 0) grid = 1;
+  }
   tet4_persistent_kernel<KT, MODE><<<grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
                                                                     k_out, f_out, dr);
   PSX_CUDA_CHECK_LAUNCH();
