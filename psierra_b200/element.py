@@ -113,10 +113,17 @@ class _GPUElementBase:
         return self._u_dev
 
     def _download(self, t: torch.Tensor, key: str) -> np.ndarray:
+        """Device tensor -> a fresh float64 numpy array (the reference returns new arrays).
+
+        The device-to-host copy lands in a reused pinned buffer; the copy out of it (with
+        the FP32 -> FP64 widening of mixed-precision K values) runs on all host threads.
+        """
         pin = self._staging.get(key, t.numel(), t.dtype)
         pin.copy_(t, non_blocking=True)
         torch.cuda.current_stream().synchronize()
-        return pin.numpy().astype(np.float64, copy=True)
+        out = torch.empty(t.numel(), dtype=torch.float64)
+        out.copy_(pin)
+        return out.numpy()
 
     def _csr(self, kvals: torch.Tensor) -> spsp.csr_matrix:
         p = self._asm.pattern
