@@ -37,6 +37,13 @@ WORKLOAD = ("cube 80^3 Kuhn Tet4 (3,072,000 elements, 531,441 nodes), NeoHookean
             "u=0.05 sin(pi x) sin(pi y) z e_z + U(+-1e-4); one fused f_int+K_T assembly per step")
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch, from one ncu
+# capture of the FP32-mixed f+K and K.v launches on the cube 56^3 (1,053,696 elements);
+# the traffic grows with the element count, so it is scaled by E for this workload.
+NCU_CAPTURE_ELEMENTS = 1053696
+NCU_TRAFFIC = {"fk32": 93.167104e6 + 73.640192e6, "kv32": 60.4928e6 + 2.330624e6}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,7 +346,10 @@ def main():
                              "K.v: 512 MB L2 flush before every timed step",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "traffic": None, "peak_kind": peak_kind,
+                         "traffic": NCU_TRAFFIC["fk32"] * E / NCU_CAPTURE_ELEMENTS,
+                         "traffic_note": "bytes per launch: ncu DRAM read+write of the cube 56^3 launch scaled by "
+                                         "elements (latency-bound: DRAM throughput 5.5% in that capture)",
+                         "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": bytes_mixed, "kernel": "tet4_persistent_kernel<float> F|K (element tiles + owner-computes gather)",
                          "launches_per_step": asm.launches_per_call("fp32-mixed")},
             "fp64": {"value": world * E / (ms_fp64 * 1e-3), "unit": "elements/s", "ms_per_step": ms_fp64,
@@ -347,6 +357,7 @@ def main():
                      "frac": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9 / peak},
             "mixed_over_fp64": ms_fp64 / ms_mixed,
             "kv": {"unit": "GB/s", "algorithmic_bytes_per_launch": bytes_kv,
+                   "traffic": NCU_TRAFFIC["kv32"] * E / NCU_CAPTURE_ELEMENTS,
                    "fp32_mixed": {"ms": ms_kv32, "gbs": bytes_kv / (ms_kv32 * 1e-3) / 1e9,
                                   "frac": bytes_kv / (ms_kv32 * 1e-3) / 1e9 / peak,
                                   "elements_per_s": world * E / (ms_kv32 * 1e-3)},
