@@ -251,6 +251,20 @@ int psx_tet10_element_dets(const int32_t* conn, const double* X, const double* u
                            double* out8, void* stream);
 
 /*
+ * Dynamic effective tangent in one sweep: K_eff = c_t K_T(u) + c_m M + c_0 K_0 with M the
+ * consistent mass of density rho (element/tet4_base.py:138-151) and K_0 the small-strain
+ * stiffness (lam, mu; or lambda_e = kappa_e - 2/3 mu_e, mu_e per element) -- the
+ * combination NonlinearDynamicAnalysis forms on the host (analysis/nonlinear_dynamic.py:
+ * 640-644, with Rayleigh damping C = alpha M + beta K_0 folded into c_m and c_0).  mode:
+ * PSX_WANT_K, optionally | PSX_WANT_F (f_out = f_int(u)).  Same CSR order, workspace and
+ * status as psx_tet4_assemble.
+ */
+int psx_tet4_assemble_effective(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
+                                const double* kappa_e, double mu, double kappa, double lam, double rho, double c_t,
+                                double c_m, double c_0, int mode, int precision, double* f_out, void* k_out,
+                                void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
  * Matrix-free tangent product y = K_T(u) v (no matrix is formed): each element
  * evaluates K_e v_e from its kinematics in closed form and the node gather sums the
  * contributions in fixed order, so y equals the assembled K_T @ v of the reference

@@ -64,6 +64,8 @@ SIGNATURES: dict[str, list] = {
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_pcg_enqueue": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_segment_sumsq": [_i64, _p, _p, _p, _p],
+    "psx_tet4_assemble_effective": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _f64, _f64, _f64, _f64, _i32, _i32, _p, _p,
+                                    _p, _i64, _p, _p],
     "psx_tile_plan_fill": [_p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p],
     "psx_tile_meta_stride": [_i32],
 }

@@ -160,6 +160,40 @@ class GPUAssembler:
             self.raise_on_bad_elements(u)
         return (f_out if want_f else None), (k_out if want_k else None)
 
+    def assemble_effective(self, u: torch.Tensor, c_t: float, c_m: float, c_0: float = 0.0, rho: float | None = None,
+                           want_f: bool = True, precision: str | None = None, f_out: torch.Tensor | None = None,
+                           k_out: torch.Tensor | None = None, check_status: bool = True):
+        """``(f_int(u), c_t K_T(u) + c_m M + c_0 K_0)`` from one sweep (Tet4).
+
+        The dynamic effective tangent of ``NonlinearDynamicAnalysis``
+        (psierra ``analysis/nonlinear_dynamic.py:640-644``): with generalized-alpha
+        constants, ``c_t = 1 - alpha_f``, ``c_m = (1 - alpha_m) a0 + (1 - alpha_f) a1 alpha_R``
+        and ``c_0 = (1 - alpha_f) a1 beta_R`` for Rayleigh damping ``alpha_R M + beta_R K_0``.
+        ``M`` is the consistent mass of density ``rho`` (default: the material's) and ``K_0``
+        the small-strain stiffness of the material.
+        """
+        if self.npe != 4:
+            raise NotImplementedError("the fused effective tangent is a Tet4 sweep")
+        prec = precision or self.precision
+        u = self._check_u(u)
+        if want_f and f_out is None:
+            f_out = self.new_f()
+        if k_out is None:
+            k_out = self.new_k(prec)
+        if k_out.dtype != self.k_dtype(prec):
+            raise ValueError(f"k_out must be {self.k_dtype(prec)} for precision {prec}")
+        self.status.zero_()
+        work = self.workspace(prec)
+        mode = _lib.PSX_WANT_K | (_lib.PSX_WANT_F if want_f else 0)
+        check(lib().psx_tet4_assemble_effective(
+            ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u), ptr(self.mu_e), ptr(self.kappa_e), self.mu, self.kappa,
+            self.lam, self.rho if rho is None else float(rho), float(c_t), float(c_m), float(c_0), mode, PRECISIONS[prec],
+            ptr(f_out) if want_f else None, ptr(k_out), ptr(work), work.numel(), ptr(self.status), _stream_handle()),
+            "psx_tet4_assemble_effective")
+        if check_status:
+            self.raise_on_bad_elements(u)
+        return (f_out if want_f else None), k_out
+
     def kv(self, u: torch.Tensor, v: torch.Tensor, precision: str | None = None,
            y_out: torch.Tensor | None = None, check_status: bool = True) -> torch.Tensor:
         """Matrix-free ``y = K_T(u) v`` (float64 in and out; element math in ``precision``)."""

@@ -101,9 +101,12 @@ __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
 }
 
 // contributions whose loads are issued together (kept within the register budget)
+#ifndef PSX_GATHER_BATCH32
+#define PSX_GATHER_BATCH32 4
+#endif
 template <typename KT>
 struct Batch {
-  static constexpr int n = sizeof(KT) == 4 ? 4 : 2;
+  static constexpr int n = sizeof(KT) == 4 ? PSX_GATHER_BATCH32 : 2;
 };
 
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list

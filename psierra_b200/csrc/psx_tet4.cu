@@ -30,6 +30,7 @@ namespace {
 constexpr int kThreads = 128;
 constexpr int kModeDR = 16;       // internal: PSX_KV with the fused dynamic-relaxation epilogue
 constexpr int kModeAdjoint = 64;  // internal: vector-Jacobian product of f_int
+constexpr int kModeEff = 128;     // internal: c_t K_T + c_m M + c_0 K_0 (dynamic effective tangent)
 #ifndef PSX_TET4_MIN_BLOCKS
 #define PSX_TET4_MIN_BLOCKS 2
 #endif
@@ -39,6 +40,9 @@ constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the r
 // no tangent (f only, K.v, dynamic relaxation) and the adjoint.  Chosen by timing the
 // 3.07M-element cube: more resident warps hide the element phase's latency, as long as
 // the element tile fits the budget without spilling.
+#ifndef PSX_TET4_TWO_PASS
+#define PSX_TET4_TWO_PASS 1
+#endif
 #ifndef PSX_TET4_MIN_BLOCKS_K32
 #define PSX_TET4_MIN_BLOCKS_K32 3
 #endif
@@ -112,6 +116,10 @@ struct Tet4Args {
   const double* kappa_e;
   double mu0, kappa0, lam0;
   Status* st;
+  // effective tangent (kModeEff): K_eff = c_t K_T + c_m M + c_0 K_0, M the consistent mass
+  // of density rho, K_0 the small-strain stiffness (lam0, mu0, or per element
+  // lambda = kappa_e - 2/3 mu_e, mu_e)
+  double c_t, c_m, c_0, rho;
 };
 
 // Phase A: one element -> its record.  tet4_total_lagrangian.py:77-139 (and, with
@@ -380,6 +388,59 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   }
   if constexpr (kWantK) {
     // K_ab[k][m] = p_a,k w_b,m + p_b,k h_a,m + y_a,k p_b,m + s_ab d_km
+    constexpr bool kEff = (MODE & kModeEff) != 0;
+    KT e_lam = 0, e_mu = 0, e_mass = 0;  // effective tangent: K_0 and mass coefficients
+    if constexpr (kEff) {
+      const KT ct = (KT)A.c_t;
+      tc.A *= ct;
+      tc.hb *= ct;
+      tc.c *= ct;
+      tc.phi *= ct;
+      const double mu_k = A.mu_e ? A.mu_e[e] : A.mu0;
+      const double lam_k = A.mu_e ? (A.kappa_e[e] - (2.0 / 3.0) * A.mu_e[e]) : A.lam0;
+      e_lam = (KT)(A.c_0 * G.V * lam_k);
+      e_mu = (KT)(A.c_0 * G.V * mu_k);
+      e_mass = (KT)(A.c_m * A.rho * fabs(G.V) * (1.0 / 20.0));  // element/tet4_base.py:138-151
+    }
+    // FP32 tangent staged in shared memory: the element's factors go through its own
+    // staging slot (and are read back after a compiler barrier), so none of the FP64
+    // kinematic and constitutive state is live while the ten blocks are formed; this
+    // keeps the register count of the fused f + K tile low enough for 3 blocks per SM
+    constexpr bool kTwoPass = PSX_TET4_TWO_PASS && !KGLOBAL && sizeof(KT) == 4 && !kLinear && !kMass;
+    if constexpr (kTwoPass) {
+      float* fs = reinterpret_cast<float*>(krec);
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          fs[3 * b + k] = (float)p[b][k];
+          fs[12 + 3 * b + k] = (float)q[b][k];
+          fs[24 + 3 * b + k] = (float)gk[b][k];
+        }
+      fs[36] = (float)tc.A;
+      fs[37] = (float)tc.hb;
+      fs[38] = (float)tc.c;
+      fs[39] = (float)tc.phi;
+      fs[40] = (float)e_lam;
+      fs[41] = (float)e_mu;
+      fs[42] = (float)e_mass;
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          p[b][k] = (KT)fs[3 * b + k];
+          q[b][k] = (KT)fs[12 + 3 * b + k];
+          gk[b][k] = (KT)fs[24 + 3 * b + k];
+        }
+      tc.A = (KT)fs[36];
+      tc.hb = (KT)fs[37];
+      tc.c = (KT)fs[38];
+      tc.phi = (KT)fs[39];
+      e_lam = (KT)fs[40];
+      e_mu = (KT)fs[41];
+      e_mass = (KT)fs[42];
+    }
     KT w[4][3], h[4][3], y[4][3];
 #pragma unroll
     for (int b = 0; b < 4; ++b)
@@ -395,13 +456,17 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     for (int a = 0; a < 4; ++a) {
 #pragma unroll
       for (int b = a; b < 4; ++b) {
-        const KT s = tc.phi * (gk[a][0] * gk[b][0] + gk[a][1] * gk[b][1] + gk[a][2] * gk[b][2]);
+        const KT gg = gk[a][0] * gk[b][0] + gk[a][1] * gk[b][1] + gk[a][2] * gk[b][2];
+        KT s = tc.phi * gg;
+        if constexpr (kEff) s += e_mu * gg + e_mass * (a == b ? (KT)2 : (KT)1);
         KT v[9];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-          for (int m = 0; m < 3; ++m)
+          for (int m = 0; m < 3; ++m) {
             v[3 * k + m] = p[a][k] * w[b][m] + p[b][k] * h[a][m] + y[a][k] * p[b][m] + (k == m ? s : (KT)0);
+            if constexpr (kEff) v[3 * k + m] += e_lam * gk[a][k] * gk[b][m] + e_mu * gk[b][k] * gk[a][m];
+          }
         if (b == a) {
           const KT d[6] = {v[0], v[1], v[2], v[4], v[5], v[8]};
           store_diag_block<KT, KGLOBAL>(krec + L::diag_off(a), d);
@@ -679,6 +744,31 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   if (wantK) return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_K) : PSX_T4(float, PSX_WANT_K);
   return PSX_T4(double, PSX_WANT_F);
 #undef PSX_T4
+}
+
+extern "C" int psx_tet4_assemble_effective(const psx_plan_t* plan, const double* X, const double* u,
+                                           const double* mu_e, const double* kappa_e, double mu, double kappa,
+                                           double lam, double rho, double c_t, double c_m, double c_0, int mode,
+                                           int precision, double* f_out, void* k_out, void* work, int64_t work_bytes,
+                                           void* status, void* stream) {
+  using namespace psx;
+  if (!plan || plan->npe != 4 || !X || !u || !status || !work || !k_out) return PSX_ERR_ARG;
+  if ((mode & PSX_WANT_K) == 0 || (mode & ~(PSX_WANT_F | PSX_WANT_K))) return PSX_ERR_ARG;
+  if ((mode & PSX_WANT_F) && !f_out) return PSX_ERR_ARG;
+  if ((mu_e == nullptr) != (kappa_e == nullptr)) return PSX_ERR_ARG;
+  WorkLayout W;
+  int rc = work_layout(plan, precision, work, &W, kMinBlocks, true);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < W.total_bytes) return PSX_ERR_ARG;
+  Tet4Args A{plan->conn, X, u, nullptr, nullptr, nullptr, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status),
+             c_t, c_m, c_0, rho};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  constexpr int kFK = PSX_WANT_F | PSX_WANT_K | kModeEff, kK = PSX_WANT_K | kModeEff;
+  if (mode & PSX_WANT_F)
+    return precision == PSX_FP64 ? run_tet4<double, kFK>(plan, A, W, static_cast<double*>(k_out), f_out, s)
+                                 : run_tet4<float, kFK>(plan, A, W, static_cast<float*>(k_out), f_out, s);
+  return precision == PSX_FP64 ? run_tet4<double, kK>(plan, A, W, static_cast<double*>(k_out), nullptr, s)
+                               : run_tet4<float, kK>(plan, A, W, static_cast<float*>(k_out), nullptr, s);
 }
 
 extern "C" int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,
