@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=40000, help="elements in the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tet10", action="store_true", help="skip the Tet10 assembly measurement")
     return ap.parse_args()
 
 
@@ -318,6 +319,44 @@ def main():
     peak, peak_kind = peak_hbm()
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
 
+    # Tet10: cube 30^3 Kuhn split upgraded to 10 nodes (162,000 elements, 226,981 nodes,
+    # nnz 57,014,289), E = 1e4, nu = 0.4, seeded smooth displacement
+    tet10 = None
+    if not args.no_tet10:
+        from psierra_b200 import meshgen
+        from psierra_b200.material import IsotropicElasticParameters, NeoHookean
+
+        m10 = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, 30, 30, 30))
+        p10 = IsotropicElasticParameters()
+        p10.set_from_youngs_poisson(youngs_modulus=1e4, poissons_ratio=0.4, mass_density=1000.0)
+        a10 = GPUAssembler(m10.nodes, m10.elements, NeoHookean(p10), precision="fp32-mixed", device=dev)
+        u10 = torch.from_numpy(meshgen.cube_smooth_u(m10, seed=7).reshape(-1)).to(dev)
+        f10 = a10.new_f()
+        k10s = a10.new_k("fp32-mixed")
+        k10d = a10.new_k("fp64")
+        a10.assemble(u10, precision="fp64", f_out=f10, k_out=k10d)
+        a10.assemble(u10, precision="fp32-mixed", f_out=f10, k_out=k10s)
+        err10 = float(((k10s.double() - k10d).abs().max() / k10d.abs().max()).item())
+        ms10s = time_steps(lambda: a10.assemble(u10, precision="fp32-mixed", f_out=f10, k_out=k10s, check_status=False),
+                           args.steps, args.warmup, sync_all)
+        ms10d = time_steps(lambda: a10.assemble(u10, precision="fp64", f_out=f10, k_out=k10d, check_status=False),
+                           args.steps, args.warmup, sync_all)
+        if world > 1:
+            t = torch.tensor([ms10s, ms10d], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms10s, ms10d = (float(x) for x in t.tolist())
+        E10, N10, nnz10 = m10.n_elements, m10.n_nodes, a10.nnz
+        b10s = 40 * E10 + 48 * N10 + 4 * nnz10 + 24 * N10
+        b10d = 40 * E10 + 48 * N10 + 8 * nnz10 + 24 * N10
+        tet10 = {"workload": "cube 30^3 Kuhn -> Tet10 (162,000 elements, 226,981 nodes, nnz 57,014,289), "
+                             "E=1e4 nu=0.4, one fused f_int+K_T assembly",
+                 "fp32_mixed": {"ms": ms10s, "elements_per_s": world * E10 / (ms10s * 1e-3),
+                                "gbs": b10s / (ms10s * 1e-3) / 1e9, "frac": b10s / (ms10s * 1e-3) / 1e9 / peak_hbm()[0]},
+                 "fp64": {"ms": ms10d, "elements_per_s": world * E10 / (ms10d * 1e-3),
+                          "gbs": b10d / (ms10d * 1e-3) / 1e9, "frac": b10d / (ms10d * 1e-3) / 1e9 / peak_hbm()[0]},
+                 "algorithmic_bytes_fp64": b10d, "K_mixed_vs_fp64_max_rel": err10}
+        del a10, k10s, k10d
+
     e2e = None
     if not args.no_e2e:
         el = Tet4TotalLagrangian(mat, precision="fp32-mixed", device=dev)
@@ -366,6 +405,7 @@ def main():
                             "elements_per_s": world * E / (ms_kv64 * 1e-3)},
                    "mixed_vs_fp64_rel2": kv_err},
             "accuracy": {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err},
+            "tet10": tet10,
             "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps * asm.launches_per_call("fp32-mixed"),
             "gpu_launches_note": "assembly timed region; each K.v step is one launch as well",
             "clocks": clk,
