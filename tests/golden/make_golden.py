@@ -3,7 +3,8 @@
 Run in a container that has the reference sources (``PSIERRA_REFERENCE_SRC``,
 default ``/root/reference/src``)::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py fbar_box   # one fixture that has its own seed
 
 Every output below comes from the reference's own classes (``Tet4TotalLagrangian``,
 ``Tet10TotalLagrangian``, ``NeoHookean``, ``SolidDomain``, ``NonlinearStaticAnalysis``,
@@ -32,6 +33,7 @@ from psierra.boundary.dirichlet import DirichletConstraint, DirichletManager  # 
 from psierra.boundary.load import NodalForce  # noqa: E402
 from psierra.domain.solid import SolidDomain  # noqa: E402
 from psierra.element.tet10_total_lagrangian import Tet10TotalLagrangian  # noqa: E402
+from psierra.element.tet4_fbar import Tet4Fbar  # noqa: E402
 from psierra.element.tet4_total_lagrangian import Tet4TotalLagrangian  # noqa: E402
 from psierra.material.neohookean import NeoHookean  # noqa: E402
 from psierra.material.parameters import IsotropicElasticParameters  # noqa: E402
@@ -136,9 +138,49 @@ def cantilever_problem(mesh, traction):
     return dm, f_ext, clamp
 
 
-def main():
+def fbar_fixture():
+    """Tet4Fbar (element/tet4_fbar.py) through SolidDomain on a small Kuhn box, plus
+    per-element calls with explicit J_bar values."""
+    m = meshgen.box_tet4(1.0, 0.5, 0.4, 4, 2, 2)
+    u = meshgen.cantilever_seeded_u(m, seed=99) * 3.0
+    mat = nh(1e4, 0.45)
+    el = Tet4Fbar(mat)
+    dom = SolidDomain(DuckMesh(m.nodes, m.elements), mat, el)
+    dom.update_state(u=u.ravel())
+    f = dom.assemble_internal_forces()
+    jbar = el._domain_J_bar.copy()  # J_bar at u (the u = 0 stiffness below resets it)
+    K = dom.assemble_tangent_stiffness_matrix()
+    Klin = dom.assemble_stiffness_matrix()
+    rng = np.random.default_rng(5)
+    pick = rng.choice(m.n_elements, size=6, replace=False)
+    ke, fe, jb = [], [], []
+    for e in pick:
+        J_bar = float(jbar[e]) * (1.0 + 0.01 * rng.normal())
+        k, fv = Tet4Fbar(mat).compute_nonlinear_force_and_tangent_stiffness(
+            m.nodes[m.elements[e]], u.reshape(-1, 3)[m.elements[e]], J_bar=J_bar)
+        ke.append(k)
+        fe.append(fv)
+        jb.append(J_bar)
+    return dict(nodes=m.nodes, elements=m.elements, u=u, f=f, K_data=K.data, K_indptr=K.indptr,
+                K_indices=K.indices, Klin_data=Klin.data, Klin_indptr=Klin.indptr, Klin_indices=Klin.indices,
+                J_bar=jbar, pick=pick, pick_J_bar=np.array(jb), pick_k=np.stack(ke), pick_f=np.stack(fe),
+                mu=mat.parameters.shear_modulus, kappa=mat.parameters.bulk_modulus,
+                lam=mat.parameters.lame_parameter_1)
+
+
+def main(only=None):
     rng = np.random.default_rng(20261203)
     out = {}
+    if only:
+        # fixtures that need no shared random stream can be regenerated on their own
+        gens = {"fbar_box": fbar_fixture}
+        for name in only:
+            out[name] = gens[name]()
+        for name, d in out.items():
+            path = os.path.join(HERE, f"{name}.npz")
+            np.savez_compressed(path, **d)
+            print(f"{name}: {os.path.getsize(path) / 1024:.1f} KiB")
+        return
 
     out["element_tet4"] = element_fixture(rng, 64, 4)
     out["element_tet10"] = element_fixture(rng, 16, 10)
@@ -240,6 +282,8 @@ def main():
     out["cfg1_newton"] = dict(trace=np.stack(dom1.trace), f_ext=f1e, clamp=clamp1,
                               converged=r1.converged, f_calls=dom1.f_calls)
 
+    out["fbar_box"] = fbar_fixture()
+
     for name, d in out.items():
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **d)
@@ -247,4 +291,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -74,3 +74,31 @@ def test_tet10_box_matches_reference():
     assert np.array_equal(K.indptr, g["K_indptr"]) and np.array_equal(K.indices, g["K_indices"])
     assert rel_max(K.data, g["K_data"]) < 1e-13
     assert rel_max(f, g["f"]) < 1e-11
+
+
+def test_fbar_oracle_matches_reference_fixture():
+    """oracle/tet4fbar.py against the reference Tet4Fbar run through SolidDomain."""
+    import scipy.sparse as spsp
+
+    from oracle import tet4fbar
+
+    g = golden("fbar_box")
+    nodes, el, u = g["nodes"], g["elements"], g["u"]
+    mu, kappa = float(g["mu"]), float(g["kappa"])
+    f = tet4fbar.internal_forces(nodes, el, u, mu, kappa)
+    assert np.abs(f - g["f"]).max() <= 1e-12 * np.abs(g["f"]).max()
+    K = tet4fbar.tangent(nodes, el, u, mu, kappa)
+    Kr = spsp.csr_matrix((g["K_data"], g["K_indices"], g["K_indptr"]), shape=K.shape)
+    assert np.abs((K - Kr).toarray()).max() <= 1e-12 * np.abs(Kr.data).max()
+    assert K.nnz == Kr.nnz and np.array_equal(K.indptr, Kr.indptr) and np.array_equal(K.indices, Kr.indices)
+    K0 = tet4fbar.tangent(nodes, el, np.zeros_like(u), mu, kappa)
+    K0r = spsp.csr_matrix((g["Klin_data"], g["Klin_indices"], g["Klin_indptr"]), shape=K.shape)
+    assert np.abs((K0 - K0r).toarray()).max() <= 1e-12 * np.abs(K0r.data).max()
+    H, V, v0 = tet4fbar.geometry(nodes, el)
+    _, J = tet4fbar.jacobians(el, u, H)
+    _, Jb = tet4fbar.j_bar(el, V, J, v0)
+    assert np.abs(Jb - g["J_bar"]).max() <= 1e-14
+    for i, e in enumerate(g["pick"]):
+        k, fe = tet4fbar.element_force_and_tangent(nodes[el[e]], u[el[e]], mu, kappa, float(g["pick_J_bar"][i]))
+        assert np.abs(k - g["pick_k"][i]).max() <= 1e-12 * np.abs(g["pick_k"][i]).max()
+        assert np.abs(fe - g["pick_f"][i]).max() <= 1e-12 * np.abs(g["pick_f"][i]).max()
