@@ -191,6 +191,20 @@ int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32_t tile, co
                        int32_t* node_src_t, int32_t* caps);
 
 /*
+ * F-bar plan (host; Tet4Fbar, element/tet4_fbar.py:53-118, 420-459): the two-ring graph
+ * of the one-ring graph nbr_ptr/nbr (sorted lists, self included; its CSR pattern is
+ * psx_csr_pattern(N, nbr2_ptr, nbr2, ...)), the one-ring gather items' positions in that
+ * CSR (pair_info2 4 n_pairs, node_info2 4 N, from psx_plan_fill's pair_info/node_info)
+ * and, per two-ring entry, the nodes a whose patch holds both ends with the one-ring
+ * entries of g_a at both ends (vol_ptr n_nbr2 + 1, vol_src 3 per entry: a, entry of
+ * (a, b), entry of (a, c); a ascending).  _count gives n_nbr2 and n_vol.
+ */
+int psx_fbar_plan_count(int64_t N, const int32_t* nbr_ptr, const int32_t* nbr, int64_t* n_nbr2, int64_t* n_vol);
+int psx_fbar_plan_fill(int64_t N, const int32_t* nbr_ptr, const int32_t* nbr, int64_t n_pairs,
+                       const int32_t* pair_info, const int32_t* node_info, int32_t* nbr2_ptr, int32_t* nbr2,
+                       int32_t* pair_info2, int32_t* node_info2, int32_t* vol_ptr, int32_t* vol_src);
+
+/*
  * Task queue of the persistent assembly kernel (host): for each granule g, the
  * element tiles of g followed by the gather tiles made ready by granule g-1-lag
  * (pairs when with_pairs, then nodes).  Each task is 4 int32 {kind, granule, begin, end};
@@ -263,6 +277,34 @@ int psx_tet4_assemble_effective(const psx_plan_t* plan, const double* X, const d
                                 const double* kappa_e, double mu, double kappa, double lam, double rho, double c_t,
                                 double c_m, double c_0, int mode, int precision, double* f_out, void* k_out,
                                 void* work, int64_t work_bytes, void* status, void* stream);
+
+/*
+ * Tet4Fbar f_int and tangent (replaces Tet4Fbar.assemble_internal_forces /
+ * assemble_tangent_stiffness_matrix, element/tet4_fbar.py:248-459) on the two-ring CSR
+ * (k_out: nnz2 doubles, zero where the reference's sum K_dev + K_vol has no entry).
+ * Device inputs: conn (E x 4), X, u (N x 3), the node -> element incidences (inc_ptr,
+ * inc_elem, psx_graph_fill), the one-ring graph and its block lists (psx_block_lists),
+ * the gather items of psx_plan_fill with psx_fbar_plan_fill positions, the two-ring
+ * vol lists; jbar_in (E, optional) replaces the nodal average, jbar_out (E, optional)
+ * receives the J_bar used.  work: psx_fbar_work_doubles(E, N, n_nbr) doubles.
+ * Scalar moduli only (the volumetric blocks use one bulk modulus, as the reference).
+ */
+int64_t psx_fbar_work_doubles(int64_t E, int64_t N, int64_t n_nbr);
+/*
+ * Independent Tet4Fbar elements with given J_bar (Tet4Fbar.compute_nonlinear_force_and_
+ * tangent_stiffness, element/tet4_fbar.py:147-211): X_elem, u_elem (device, n x 4 x 3),
+ * jbar (n) -> k_out (n x 12 x 12), f_out (n x 12).
+ */
+int psx_fbar_element(int64_t n, const double* X_elem, const double* u_elem, const double* jbar, double mu,
+                     double kappa, double* k_out, double* f_out, void* status, void* stream);
+int psx_fbar_assemble(const int32_t* conn, int64_t E, int64_t N, const double* X, const double* u, double mu,
+                      double kappa, const int32_t* inc_ptr, const int32_t* inc_elem, const int32_t* nbr_ptr,
+                      const int32_t* nbr, int64_t n_nbr, const int32_t* blk_ptr, const int32_t* blk_src,
+                      int64_t n_pairs, const int32_t* pair_info2, const int32_t* pair_ptr, const int32_t* pair_src,
+                      const int32_t* node_info2, const int32_t* node_ptr, const int32_t* node_src,
+                      const int32_t* nbr2_ptr, const int32_t* vol_ptr, const int32_t* vol_src, const double* jbar_in,
+                      double* f_out, double* k_out, int64_t nnz2, double* jbar_out, double* work,
+                      int64_t work_doubles, void* status, void* stream);
 
 /*
  * Matrix-free tangent product y = K_T(u) v (no matrix is formed): each element

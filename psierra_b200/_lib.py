@@ -64,6 +64,12 @@ SIGNATURES: dict[str, list] = {
     "psx_pcg": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_pcg_enqueue": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _i64, _p, _p],
     "psx_segment_sumsq": [_i64, _p, _p, _p, _p],
+    "psx_fbar_plan_count": [_i64, _p, _p, _p, _p],
+    "psx_fbar_plan_fill": [_i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _p, _p],
+    "psx_fbar_work_doubles": [_i64, _i64, _i64],
+    "psx_fbar_element": [_i64, _p, _p, _p, _f64, _f64, _p, _p, _p, _p],
+    "psx_fbar_assemble": [_p, _i64, _i64, _p, _p, _f64, _f64, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p,
+                          _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p],
     "psx_tet4_assemble_effective": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _f64, _f64, _f64, _f64, _i32, _i32, _p, _p,
                                     _p, _i64, _p, _p],
     "psx_tile_plan_fill": [_p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p],
@@ -133,6 +139,7 @@ def lib() -> ctypes.CDLL:
         L.psx_status_bytes.argtypes = []
         L.psx_status_bytes.restype = ctypes.c_size_t
         L.psx_tile_meta_stride.restype = ctypes.c_int64
+        L.psx_fbar_work_doubles.restype = ctypes.c_int64
         _lib = L
     return _lib
 

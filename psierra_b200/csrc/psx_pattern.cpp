@@ -444,6 +444,121 @@ extern "C" int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32
 }
 
 // ---------------------------------------------------------------------------
+// F-bar plan (Tet4Fbar, element/tet4_fbar.py:53-118, 420-459).  The nodal volumetric
+// blocks kappa v0_a g_a g_a^T couple every two nodes of node a's element patch, so the
+// tangent lives on the two-ring graph: b ~ c when some node a neighbours both.  For
+// each two-ring block (b, c) the plan lists the nodes a it sums over (ascending, the
+// order of the reference's COO -> CSR accumulation) with the one-ring entries of g_a[b]
+// and g_a[c]; the one-ring gather items get their positions in the two-ring CSR.
+namespace {
+inline int32_t rank_in(const int32_t* list, int32_t n, int32_t v) {
+  return (int32_t)(std::lower_bound(list, list + n, v) - list);
+}
+}  // namespace
+
+extern "C" int psx_fbar_plan_count(int64_t N, const int32_t* nbr_ptr, const int32_t* nbr, int64_t* n_nbr2,
+                                   int64_t* n_vol) {
+  if (N <= 0 || !nbr_ptr || !nbr || !n_nbr2 || !n_vol) return PSX_ERR_ARG;
+  std::vector<int32_t> mark(N, -1);
+  int64_t tot = 0, vol = 0;
+  for (int64_t b = 0; b < N; ++b) {
+    for (int32_t x = nbr_ptr[b]; x < nbr_ptr[b + 1]; ++x) {
+      const int32_t a = nbr[x];
+      for (int32_t y = nbr_ptr[a]; y < nbr_ptr[a + 1]; ++y)
+        if (mark[nbr[y]] != (int32_t)b) {
+          mark[nbr[y]] = (int32_t)b;
+          ++tot;
+        }
+    }
+  }
+  for (int64_t a = 0; a < N; ++a) {
+    const int64_t d = nbr_ptr[a + 1] - nbr_ptr[a];
+    vol += d * d;
+  }
+  if (9 * tot >= ((int64_t)1 << 31) || 3 * vol >= ((int64_t)1 << 31)) return PSX_ERR_LIMIT;
+  *n_nbr2 = tot;
+  *n_vol = vol;
+  return PSX_OK;
+}
+
+extern "C" int psx_fbar_plan_fill(int64_t N, const int32_t* nbr_ptr, const int32_t* nbr, int64_t n_pairs,
+                                  const int32_t* pair_info, const int32_t* node_info, int32_t* nbr2_ptr,
+                                  int32_t* nbr2, int32_t* pair_info2, int32_t* node_info2, int32_t* vol_ptr,
+                                  int32_t* vol_src) {
+  if (N <= 0 || !nbr_ptr || !nbr || n_pairs < 0 || !pair_info || !node_info || !nbr2_ptr || !nbr2 ||
+      !pair_info2 || !node_info2 || !vol_ptr || !vol_src)
+    return PSX_ERR_ARG;
+  // two-ring neighbour lists (sorted, self included)
+  std::vector<int32_t> tmp;
+  nbr2_ptr[0] = 0;
+  for (int64_t b = 0; b < N; ++b) {
+    tmp.clear();
+    for (int32_t x = nbr_ptr[b]; x < nbr_ptr[b + 1]; ++x) {
+      const int32_t a = nbr[x];
+      tmp.insert(tmp.end(), nbr + nbr_ptr[a], nbr + nbr_ptr[a + 1]);
+    }
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    std::copy(tmp.begin(), tmp.end(), nbr2 + nbr2_ptr[b]);
+    nbr2_ptr[b + 1] = nbr2_ptr[b] + (int32_t)tmp.size();
+  }
+  auto rank2 = [&](int32_t i, int32_t j) { return rank_in(nbr2 + nbr2_ptr[i], nbr2_ptr[i + 1] - nbr2_ptr[i], j); };
+  // one-ring gather positions -> two-ring CSR positions
+  for (int64_t k = 0; k < n_pairs; ++k) {
+    const int32_t pos = pair_info[4 * k];
+    // row node i: 9 nbr_ptr[i] <= pos < 9 nbr_ptr[i + 1]
+    const int32_t i = (int32_t)(std::upper_bound(nbr_ptr, nbr_ptr + N + 1, pos / 9) - nbr_ptr) - 1;
+    const int32_t r = (pos - 9 * nbr_ptr[i]) / 3;
+    const int32_t j = nbr[nbr_ptr[i] + r];
+    const int32_t deg2i = nbr2_ptr[i + 1] - nbr2_ptr[i], deg2j = nbr2_ptr[j + 1] - nbr2_ptr[j];
+    pair_info2[4 * k + 0] = 9 * nbr2_ptr[i] + 3 * rank2(i, j);
+    pair_info2[4 * k + 1] = 3 * deg2i;
+    pair_info2[4 * k + 2] = 9 * nbr2_ptr[j] + 3 * rank2(j, i);
+    pair_info2[4 * k + 3] = 3 * deg2j;
+  }
+  for (int64_t k = 0; k < N; ++k) {
+    const int32_t i = node_info[4 * k + 2];
+    const int32_t deg2i = nbr2_ptr[i + 1] - nbr2_ptr[i];
+    node_info2[4 * k + 0] = 9 * nbr2_ptr[i] + 3 * rank2(i, i);
+    node_info2[4 * k + 1] = node_info[4 * k + 1] > 0 ? 3 * deg2i : 0;
+    node_info2[4 * k + 2] = i;
+    node_info2[4 * k + 3] = 0;
+  }
+  // volumetric lists: for block (b, c), the common one-ring neighbours a of b and c
+  int64_t out = 0;
+  vol_ptr[0] = 0;
+  for (int64_t b = 0; b < N; ++b) {
+    const int32_t* nb = nbr + nbr_ptr[b];
+    const int32_t db = nbr_ptr[b + 1] - nbr_ptr[b];
+    for (int32_t t = nbr2_ptr[b]; t < nbr2_ptr[b + 1]; ++t) {
+      const int32_t c = nbr2[t];
+      const int32_t* nc = nbr + nbr_ptr[c];
+      const int32_t dc = nbr_ptr[c + 1] - nbr_ptr[c];
+      int32_t x = 0, y = 0;
+      while (x < db && y < dc) {
+        if (nb[x] < nc[y]) {
+          ++x;
+        } else if (nb[x] > nc[y]) {
+          ++y;
+        } else {
+          const int32_t a = nb[x];
+          const int32_t* na = nbr + nbr_ptr[a];
+          const int32_t da = nbr_ptr[a + 1] - nbr_ptr[a];
+          vol_src[3 * out + 0] = a;
+          vol_src[3 * out + 1] = nbr_ptr[a] + rank_in(na, da, (int32_t)b);
+          vol_src[3 * out + 2] = nbr_ptr[a] + rank_in(na, da, c);
+          ++out;
+          ++x;
+          ++y;
+        }
+      }
+      vol_ptr[t + 1] = (int32_t)out;
+    }
+  }
+  return PSX_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Task queue of the persistent assembly kernel: for each granule g, the element
 // tiles of g followed by the gather tiles made ready by granule g-1-lag (pairs, then
 // nodes); the gather tiles of the last granules close the queue.  The lag keeps gather

@@ -241,3 +241,104 @@ class Tet10TotalLagrangian(_GPUElementBase):
 
     def assemble_mass_matrix(self, mesh):
         raise NotImplementedError("the Tet10 consistent mass is assembled by SolidDomain.assemble_mass_matrix")
+
+
+class Tet4Fbar(_GPUElementBase):
+    """GPU Tet4 F-bar element (psierra ``element/tet4_fbar.py``): nodal volume-averaged
+    ``J_bar``, deviatoric element tangent and nodal volumetric blocks on the two-ring
+    pattern (``psierra_b200.fbar``).  Same domain hooks and return types as the reference
+    class; the tangent's CSR pattern is the reference's (scipy's ``K_dev + K_vol``, exact
+    zeros dropped)."""
+
+    _npe = 4
+
+    def __init__(self, material, device=None) -> None:
+        super().__init__(material, precision="fp64", device=device)
+        self._fbar = None
+        self._domain_J_bar: np.ndarray | None = None
+
+    def _make_assembler(self, mesh):
+        from psierra_b200.fbar import FbarAssembler
+
+        self._fbar = FbarAssembler(mesh.nodes, mesh.elements, self._material, device=self.device)
+        return self._fbar
+
+    @property
+    def material(self):
+        return self._material
+
+    @material.setter
+    def material(self, mat) -> None:
+        self._material = mat
+        self._mesh = None  # moduli are baked into the assembler
+        self._asm = None
+
+    def _setup(self, mesh):
+        if self._mesh is not mesh or self._asm is None:
+            elements = np.asarray(mesh.elements)
+            if elements.ndim != 2 or elements.shape[1] != 4:
+                raise ValueError(f"Tet4Fbar needs (E, 4) elements, got {elements.shape}")
+            self._asm = self._make_assembler(mesh)
+            self._mesh = mesh
+            self._u_dev = torch.empty(3 * self._asm.n_nodes, dtype=torch.float64, device=self._asm.device)
+        return self._asm
+
+    def _record_jbar(self) -> None:
+        self._domain_J_bar = self._fbar.jbar.cpu().numpy().copy()
+
+    def prepare_for_assembly(self, mesh, displacement=None) -> None:
+        """Mesh setup and the nodal-averaged J_bar (psierra ``tet4_fbar.py:213-243``)."""
+        asm = self._setup(mesh)
+        if displacement is not None:
+            asm.assemble(self._upload_u(displacement), want_f=True, want_k=False)
+            self._record_jbar()
+
+    def assemble_internal_forces(self, mesh, displacement) -> np.ndarray:
+        asm = self._setup(mesh)
+        f, _ = asm.assemble(self._upload_u(displacement), want_f=True, want_k=False)
+        self._record_jbar()
+        return self._download(f, "f")
+
+    def assemble_tangent_stiffness_matrix(self, mesh, displacement) -> spsp.csr_matrix:
+        asm = self._setup(mesh)
+        _, k = asm.assemble(self._upload_u(displacement), want_f=False, want_k=True)
+        self._record_jbar()
+        return asm.csr(k)
+
+    def assemble_force_and_tangent(self, mesh, displacement):
+        asm = self._setup(mesh)
+        f, k = asm.assemble(self._upload_u(displacement), want_f=True, want_k=True)
+        self._record_jbar()
+        return self._download(f, "f"), asm.csr(k)
+
+    def assemble_stiffness_matrix(self, mesh) -> spsp.csr_matrix:
+        """The tangent at zero displacement (psierra ``tet4_fbar.py:241-246``)."""
+        asm = self._setup(mesh)
+        return self.assemble_tangent_stiffness_matrix(mesh, np.zeros((asm.n_nodes, 3)))
+
+    def assemble_mass_matrix(self, mesh) -> spsp.csr_matrix:
+        return Tet4TotalLagrangian(self._material, device=self.device).assemble_mass_matrix(mesh)
+
+    def compute_mass_matrix(self, volume: float) -> np.ndarray:
+        return Tet4TotalLagrangian(self._material, device=self.device).compute_mass_matrix(volume)
+
+    def compute_linear_stiffness_matrix(self, node_coords, elem_index=None, **kw):
+        return Tet4TotalLagrangian(self._material, device=self.device).compute_linear_stiffness_matrix(node_coords)
+
+    def compute_nonlinear_force_and_tangent_stiffness(self, node_coords, u_nodes, elem_index=None, J_bar=None, **kw):
+        """(k_tan 12x12, f_int 12) of one element (psierra ``tet4_fbar.py:147-211``)."""
+        from psierra_b200.fbar import FbarAssembler
+
+        X = np.asarray(node_coords, dtype=np.float64).reshape(4, 3)
+        un = np.asarray(u_nodes, dtype=np.float64).reshape(4, 3)
+        if J_bar is None:
+            if elem_index is not None and self._domain_J_bar is not None:
+                J_bar = float(self._domain_J_bar[elem_index])
+            else:
+                A = np.ones((4, 4))
+                A[:, 1:] = X
+                H = np.linalg.inv(A)[1:, :].T
+                J_bar = float(np.linalg.det(np.eye(3) + un.T @ H))
+        one = FbarAssembler(X, np.arange(4, dtype=np.int64)[None, :], self._material, device=self.device)
+        k, f = one.element_matrices(X[None], un[None], np.array([J_bar]))
+        return k[0], f[0]

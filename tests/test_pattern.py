@@ -133,3 +133,38 @@ def test_pattern_rejects_bad_connectivity():
         MeshPattern(els, 4)
     with pytest.raises(ValueError):
         MeshPattern(np.zeros((3, 5), dtype=np.int64), 8)
+
+
+def test_fbar_plan_two_ring_and_volumetric_lists():
+    """psx_fbar_plan_fill: two-ring lists and the common-neighbour lists of every block."""
+    import ctypes
+
+    from psierra_b200._lib import check, lib, ptr
+    from psierra_b200.pattern import MeshPattern
+
+    m = MESHES["unstructured"]()
+    p = MeshPattern(m.elements, m.n_nodes)
+    h = p.plan_host()
+    N = m.n_nodes
+    n2, nv = ctypes.c_int64(), ctypes.c_int64()
+    check(lib().psx_fbar_plan_count(N, ptr(p.nbr_ptr), ptr(p.nbr), ctypes.byref(n2), ctypes.byref(nv)), "count")
+    nbr2_ptr = np.zeros(N + 1, dtype=np.int32)
+    nbr2 = np.zeros(int(n2.value), dtype=np.int32)
+    pi2 = np.zeros(4 * h["n_pairs"], dtype=np.int32)
+    ni2 = np.zeros(4 * N, dtype=np.int32)
+    vptr = np.zeros(int(n2.value) + 1, dtype=np.int32)
+    vsrc = np.zeros(3 * int(nv.value), dtype=np.int32)
+    check(lib().psx_fbar_plan_fill(N, ptr(p.nbr_ptr), ptr(p.nbr), h["n_pairs"], ptr(h["pair_info"]), ptr(h["node_info"]),
+                                   ptr(nbr2_ptr), ptr(nbr2), ptr(pi2), ptr(ni2), ptr(vptr), ptr(vsrc)), "fill")
+    ring1 = [set(p.nbr[p.nbr_ptr[i]:p.nbr_ptr[i + 1]].tolist()) for i in range(N)]
+    for b in range(N):
+        want = sorted(set().union(*(ring1[a] for a in ring1[b])))
+        got = nbr2[nbr2_ptr[b]:nbr2_ptr[b + 1]].tolist()
+        assert got == want
+        for t in range(nbr2_ptr[b], nbr2_ptr[b + 1]):
+            c = int(nbr2[t])
+            entries = vsrc[3 * vptr[t]:3 * vptr[t + 1]].reshape(-1, 3)
+            assert entries[:, 0].tolist() == sorted(ring1[b] & ring1[c])
+            for a, qab, qac in entries:
+                assert p.nbr[qab] == b and p.nbr[qac] == c and p.nbr_ptr[a] <= qab < p.nbr_ptr[a + 1]
+    assert int(nv.value) == sum(len(r) ** 2 for r in ring1)
