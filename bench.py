@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tet10", action="store_true", help="skip the Tet10 assembly measurement")
+    ap.add_argument("--no-fbar", action="store_true", help="skip the Tet4Fbar assembly measurement")
     return ap.parse_args()
 
 
@@ -357,6 +358,30 @@ def main():
                  "algorithmic_bytes_fp64": b10d, "K_mixed_vs_fp64_max_rel": err10}
         del a10, k10s, k10d
 
+    # Tet4Fbar: cube 30^3 Kuhn (162,000 Tet4), E = 1e4, nu = 0.49, seeded smooth displacement;
+    # f_int + tangent on the two-ring pattern (the reference's K_dev + K_vol)
+    fbar = None
+    if not args.no_fbar:
+        from psierra_b200 import meshgen
+        from psierra_b200.fbar import FbarAssembler
+        from psierra_b200.material import IsotropicElasticParameters, NeoHookean
+
+        mf = meshgen.box_tet4(1.0, 1.0, 1.0, 30, 30, 30)
+        pf = IsotropicElasticParameters()
+        pf.set_from_youngs_poisson(youngs_modulus=1e4, poissons_ratio=0.49, mass_density=1000.0)
+        af = FbarAssembler(mf.nodes, mf.elements, NeoHookean(pf), device=dev)
+        uf = torch.from_numpy(meshgen.cube_smooth_u(mf, seed=11).reshape(-1)).to(dev)
+        af.assemble(uf)
+        msf = time_steps(lambda: af.assemble(uf, check_status=False), args.steps, args.warmup, sync_all)
+        if world > 1:
+            t = torch.tensor([msf], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            msf = float(t.item())
+        fbar = {"workload": "cube 30^3 Kuhn Tet4Fbar (162,000 elements, 29,791 nodes), E=1e4 nu=0.49, "
+                            "f_int + K_dev + K_vol on the two-ring pattern",
+                "ms": msf, "elements_per_s": world * mf.n_elements / (msf * 1e-3), "nnz_two_ring": af.nnz}
+        del af
+
     e2e = None
     if not args.no_e2e:
         el = Tet4TotalLagrangian(mat, precision="fp32-mixed", device=dev)
@@ -406,6 +431,7 @@ def main():
                    "mixed_vs_fp64_rel2": kv_err},
             "accuracy": {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err},
             "tet10": tet10,
+            "fbar": fbar,
             "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps * asm.launches_per_call("fp32-mixed"),
             "gpu_launches_note": "assembly timed region; each K.v step is one launch as well",
             "clocks": clk,
