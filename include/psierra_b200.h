@@ -307,6 +307,20 @@ int psx_fbar_assemble(const int32_t* conn, int64_t E, int64_t N, const double* X
                       int64_t work_doubles, void* status, void* stream);
 
 /*
+ * Hyper-reduced (ECSW) Tet4 evaluation (replaces HyperReducedECSWModel.
+ * evaluate_forces_and_stiffness, hyperreduction/model.py:254-318): for the n elements of
+ * the reduced integration domain -- reference coordinates X_elem (n x 4 x 3), modal
+ * sub-bases phi_elem (n x 12 x r, row-major), cubature weights (n), optional per-element
+ * moduli (n) -- and reduced coordinates u_r (r): f_r (r) = sum_e w_e Phi_e^T f_e(Phi_e u_r)
+ * and K_r (r x r) = sym(sum_e w_e Phi_e^T k_e(Phi_e u_r) Phi_e), summed in element order.
+ * work: psx_ecsw_work_doubles(n, r) doubles.  Status as psx_tet4_assemble.
+ */
+int64_t psx_ecsw_work_doubles(int64_t n, int32_t r);
+int psx_ecsw_evaluate(int64_t n, int32_t r, const double* X_elem, const double* phi_elem, const double* weights,
+                      const double* u_r, const double* mu_e, const double* kappa_e, double mu, double kappa,
+                      double* f_r, double* K_r, double* work, int64_t work_doubles, void* status, void* stream);
+
+/*
  * Matrix-free tangent product y = K_T(u) v (no matrix is formed): each element
  * evaluates K_e v_e from its kinematics in closed form and the node gather sums the
  * contributions in fixed order, so y equals the assembled K_T @ v of the reference

@@ -68,6 +68,8 @@ SIGNATURES: dict[str, list] = {
     "psx_fbar_plan_fill": [_i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _p, _p],
     "psx_fbar_work_doubles": [_i64, _i64, _i64],
     "psx_fbar_element": [_i64, _p, _p, _p, _f64, _f64, _p, _p, _p, _p],
+    "psx_ecsw_work_doubles": [_i64, _i32],
+    "psx_ecsw_evaluate": [_i64, _i32, _p, _p, _p, _p, _p, _p, _f64, _f64, _p, _p, _p, _i64, _p, _p],
     "psx_fbar_assemble": [_p, _i64, _i64, _p, _p, _f64, _f64, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p,
                           _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p],
     "psx_tet4_assemble_effective": [_p, _p, _p, _p, _p, _f64, _f64, _f64, _f64, _f64, _f64, _f64, _i32, _i32, _p, _p,
@@ -140,6 +142,7 @@ def lib() -> ctypes.CDLL:
         L.psx_status_bytes.restype = ctypes.c_size_t
         L.psx_tile_meta_stride.restype = ctypes.c_int64
         L.psx_fbar_work_doubles.restype = ctypes.c_int64
+        L.psx_ecsw_work_doubles.restype = ctypes.c_int64
         _lib = L
     return _lib
 
