@@ -45,6 +45,27 @@ def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+def partition_instances(sizes, world: int) -> list[np.ndarray]:
+    """Split a batch across ``world`` ranks (one GPU each), balanced by element count.
+
+    Instances are independent, so each rank solves its own share with no collective on
+    the data path.  Greedy longest-processing-time assignment in a fixed order (sizes
+    descending, ties by index), so every rank computes the same partition; each rank's
+    indices are returned ascending.
+    """
+    sizes = np.asarray(sizes, dtype=np.int64)
+    if world <= 0:
+        raise ValueError("world must be positive")
+    order = np.lexsort((np.arange(sizes.size), -sizes))
+    load = np.zeros(world, dtype=np.int64)
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = int(np.argmin(load))  # lowest rank wins ties
+        parts[r].append(int(i))
+        load[r] += sizes[i]
+    return [np.array(sorted(p), dtype=np.int64) for p in parts]
+
+
 class MeshBatch:
     """Disjoint union of Tet4 meshes with per-instance (or per-element) NeoHookean moduli."""
 
