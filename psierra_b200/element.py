@@ -17,6 +17,8 @@ the device and widened to float64 on the way out; f_int stays FP64.
 """
 from __future__ import annotations
 
+import weakref
+
 import numpy as np
 import scipy.sparse as spsp
 import torch
@@ -39,6 +41,47 @@ class _HostStaging:
         return b[:n]
 
 
+class _ResultPool:
+    """Pinned float64 buffers handed out as the backing store of returned arrays.
+
+    A device result is copied straight into a free pinned buffer and returned as a numpy
+    view of it; a finalizer on that array returns the buffer to the pool once the caller
+    holds no reference to it any more.  Every call therefore still returns a fresh array
+    that no other live result aliases (the reference's semantics), without a host-side
+    copy.  Past ``cap_bytes`` of buffers in use, results fall back to freshly allocated
+    (pageable) arrays.
+    """
+
+    def __init__(self, cap_bytes: int = 8 << 30):
+        self.cap = cap_bytes
+        self.free: list[torch.Tensor] = []
+        self.in_use_bytes = 0
+
+    def _release(self, buf: torch.Tensor) -> None:
+        self.in_use_bytes -= buf.numel() * 8
+        self.free.append(buf)
+
+    def take(self, dev: torch.Tensor) -> np.ndarray:
+        n = dev.numel()
+        buf = None
+        for i, b in enumerate(self.free):
+            if b.numel() == n:
+                buf = self.free.pop(i)
+                break
+        if buf is None:
+            if self.in_use_bytes + 8 * n > self.cap:
+                out = torch.empty(n, dtype=torch.float64)
+                out.copy_(dev)
+                return out.numpy()
+            buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        self.in_use_bytes += 8 * n
+        buf.copy_(dev, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        arr = buf.numpy()
+        weakref.finalize(arr, self._release, buf)
+        return arr
+
+
 class _GPUElementBase:
     """Common host <-> device plumbing of the drop-in element classes."""
 
@@ -52,6 +95,8 @@ class _GPUElementBase:
         self._mesh = None
         self._asm: GPUAssembler | None = None
         self._staging = _HostStaging()
+        self._results = _ResultPool()
+        self._widen: torch.Tensor | None = None
         self._u_dev: torch.Tensor | None = None
         self._last_u: np.ndarray | None = None
         self._last_f: torch.Tensor | None = None
@@ -125,9 +170,19 @@ class _GPUElementBase:
         out.copy_(pin)
         return out.numpy()
 
+    def _download_k(self, kvals: torch.Tensor) -> np.ndarray:
+        """CSR values -> a fresh float64 host array: FP32 values are widened on the device,
+        then copied once into a pooled pinned buffer (``_ResultPool``)."""
+        if kvals.dtype != torch.float64:
+            if self._widen is None or self._widen.numel() != kvals.numel():
+                self._widen = torch.empty(kvals.numel(), dtype=torch.float64, device=kvals.device)
+            self._widen.copy_(kvals)
+            kvals = self._widen
+        return self._results.take(kvals)
+
     def _csr(self, kvals: torch.Tensor) -> spsp.csr_matrix:
         p = self._asm.pattern
-        data = self._download(kvals, "k")
+        data = self._download_k(kvals)
         n = p.n_dofs
         A = spsp.csr_matrix((data, p.indices, p.indptr), shape=(n, n), copy=False)
         A.has_sorted_indices = True
