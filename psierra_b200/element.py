@@ -195,7 +195,7 @@ class _GPUElementBase:
         asm = self._setup(mesh)
         u = self._upload_u(displacement)
         f, _ = asm.assemble(u, want_f=True, want_k=False)
-        return self._download(f, "f")
+        return self._results.take(f)
 
     def assemble_tangent_stiffness_matrix(self, mesh, displacement) -> spsp.csr_matrix:
         """K_T(u) as a canonical CSR matrix (psierra ``domain/solid.py:280-325``)."""
@@ -221,7 +221,7 @@ class _GPUElementBase:
         asm = self._setup(mesh)
         u = self._upload_u(displacement)
         f, k = asm.assemble(u, want_f=True, want_k=True)
-        return self._download(f, "f"), self._csr(k)
+        return self._results.take(f), self._csr(k)
 
     # ---------------------------------------------------------------- per-element API
     def compute_nonlinear_force_and_tangent_stiffness(self, node_coords, u_nodes, elem_index=None, **kw):

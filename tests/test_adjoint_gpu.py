@@ -125,3 +125,47 @@ def test_shear_modulus_identification_lowers_the_misfit():
     # 96 per-element moduli from one load case: under-determined, so only the misfit is checked
     assert min(hist) < 0.2 * hist[0]
     assert np.all(np.isfinite(mu_fit)) and np.all(mu_fit > 0)
+
+
+def test_ellipsoid_gravity_identification_gradient():
+    """The ellipsoid workload at a coarse spacing: gravity through the consistent mass,
+    clamp z < -0.06, mu_e ~ LogNormal(ln 1000, 0.3), kappa = 50 mu; the gradient of the
+    displacement misfit against a second seed's solution, checked by central differences
+    (h = 1e-4 mu_e) on random elements.  Loaded to 20 % of gravity: the soft body resting
+    on its small clamped cap loses static stability (it starts to tip) near a third of
+    the full load, where no nearby equilibrium exists for Newton to find."""
+    import scipy.sparse as spsp
+
+    m = meshgen.ellipsoid_tet4(0.08, 0.06, 0.07, 0.012)
+    rng = np.random.default_rng(41)
+    mu_t = np.exp(np.log(1000.0) + 0.3 * rng.normal(size=m.n_elements))
+    mu0 = np.exp(np.log(1000.0) + 0.3 * np.random.default_rng(42).normal(size=m.n_elements))
+    asm = GPUAssembler(m.nodes, m.elements, NeoHookeanField(mu0, 50.0 * mu0, mass_density=1040.0))
+    _, mv = asm.assemble(None, mass=True)
+    M = spsp.csr_matrix((mv.cpu().numpy(), asm.pattern.indices, asm.pattern.indptr), shape=(m.n_dofs,) * 2)
+    gvec = np.tile([0.0, 0.0, -9.81], m.n_nodes)
+    f_ext = torch.from_numpy(0.2 * (M @ gvec)).to(DEV)
+    fixed_nodes = np.where(m.nodes[:, 2] < -0.06 + 1e-12)[0]
+    assert fixed_nodes.size > 3
+    fixed = np.concatenate([3 * fixed_nodes + c for c in range(3)])
+    nt = DeviceNewton(asm, fixed, precision="fp64", pcg_tol=1e-13)
+    with torch.no_grad():
+        mt = torch.from_numpy(mu_t).to(DEV)
+        u_tgt = static_equilibrium(nt, mt, 50.0 * mt, f_ext, n_steps=2, polish=3)
+
+    def loss_of(mu_np):
+        mv_ = torch.from_numpy(mu_np).to(DEV).requires_grad_(True)
+        u = static_equilibrium(nt, mv_, 50.0 * mv_, f_ext, n_steps=2, polish=3)
+        return 0.5 * torch.sum((u - u_tgt) ** 2), mv_
+
+    L, mv_ = loss_of(mu0)
+    L.backward()
+    g = mv_.grad.cpu().numpy()
+    for e in rng.choice(m.n_elements, size=8, replace=False):
+        h = 1e-4 * mu0[e]
+        mp, mm = mu0.copy(), mu0.copy()
+        mp[e] += h
+        mm[e] -= h
+        with torch.no_grad():
+            fd = (float(loss_of(mp)[0]) - float(loss_of(mm)[0])) / (2 * h)
+        assert abs(g[e] - fd) <= 1e-5 * abs(fd) + 1e-12 * abs(float(L.detach())), (e, g[e], fd)
