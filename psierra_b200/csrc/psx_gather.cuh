@@ -100,18 +100,21 @@ __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
   }
 }
 
-// contributions whose loads are issued together (kept within the register budget)
-#ifndef PSX_GATHER_BATCH32
-#define PSX_GATHER_BATCH32 4
-#endif
-template <typename KT>
-struct Batch {
-  static constexpr int n = sizeof(KT) == 4 ? PSX_GATHER_BATCH32 : 2;
+// Contributions whose loads are issued together, kept within the register budget: the
+// fused FP32 f + K Tet4 kernel runs 3 blocks per SM, which its 168 registers allow only
+// with two pair and one node contribution in flight; the other sweeps keep four.
+template <typename KT, int NPE, bool WANT_K, bool WANT_F>
+struct PairBatch {
+  static constexpr int n = sizeof(KT) == 8 ? 2 : (NPE == 4 && WANT_K && WANT_F ? 2 : 4);
+};
+template <typename KT, int NPE, bool WANT_K, bool WANT_F>
+struct NodeBatch {
+  static constexpr int n = sizeof(KT) == 8 ? 2 : (NPE == 4 && WANT_K && WANT_F ? 1 : 4);
 };
 
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list
 // (ascending element) order; their loads are issued kBatch at a time.
-template <typename KT, int NPE, bool TILES = false>
+template <typename KT, int NPE, bool TILES = false, bool WANT_F = false>
 __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, const KT* __restrict__ krec,
                                             KT* __restrict__ k_out) {
   using L = RecLayout<NPE>;
@@ -122,7 +125,7 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
   KT acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = (KT)0;
-  constexpr int kBatch = Batch<KT>::n;
+  constexpr int kBatch = PairBatch<KT, NPE, true, WANT_F>::n;
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
@@ -177,7 +180,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc[j] = (KT)0;
   double fa[3] = {0.0, 0.0, 0.0};
-  constexpr int kBatch = Batch<KT>::n;
+  constexpr int kBatch = NodeBatch<KT, NPE, WANT_K, WANT_F>::n;
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
@@ -365,7 +368,7 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
       __syncwarp();
       for (int32_t item = task.z + lane; item < task.w; item += 32) {
         if (task.x == 1) {
-          if constexpr (WANT_K) gather_pair<KT, NPE, TILES>(g, item, krec, k_out);
+          if constexpr (WANT_K) gather_pair<KT, NPE, TILES, WANT_F>(g, item, krec, k_out);
         } else {
           gather_node<KT, NPE, WANT_K, WANT_F, DR, TILES>(g, item, krec, frec, k_out, f_out, &dr);
         }

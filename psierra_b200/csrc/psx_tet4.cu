@@ -33,7 +33,7 @@ constexpr int kModeDR = 16;       // internal: PSX_KV with the fused dynamic-rel
 constexpr int kModeAdjoint = 64;  // internal: vector-Jacobian product of f_int
 constexpr int kModeEff = 128;     // internal: c_t K_T + c_m M + c_0 K_0 (dynamic effective tangent)
 #ifndef PSX_TET4_MIN_BLOCKS
-#define PSX_TET4_MIN_BLOCKS 2
+#define PSX_TET4_MIN_BLOCKS 3
 #endif
 constexpr int kMinBlocks = PSX_TET4_MIN_BLOCKS;  // resident blocks per SM the register budget targets
 // Register targets of the other instantiations (resident blocks per SM, which is also

@@ -76,7 +76,7 @@ class MeshPattern:
     # the K queue, lag of the f / K.v queue (granules), ring slack (granules; 0 = 6).  The
     # Tet4 values are the fastest of a lag x slack sweep on the 3.07M-element cube
     # (FP32-mixed f+K and f / K.v timed separately).
-    QUEUE = {4: (4096, 32, 32, 12, 16, 12), 10: (512, 8, 32, 16, 16, 0)}
+    QUEUE = {4: (4096, 32, 32, 20, 16, 12), 10: (512, 8, 32, 16, 16, 0)}
 
     def plan_host(self) -> dict:
         """Host arrays of the gather plan (``psx_plan_fill``), built once."""
