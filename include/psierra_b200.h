@@ -392,6 +392,15 @@ int psx_pcg_enqueue(int64_t n, const int32_t* indptr, const int32_t* indices, co
                     int precond, void* work, int64_t work_bytes, void* status, void* stream);
 
 /*
+ * y = alpha A x + beta y for a CSR matrix (values double for PSX_FP64, float for
+ * PSX_FP32_MIXED; x, y double, device), rows summed in a fixed order: the products with
+ * the constant mass and stiffness matrices in the dynamic residual
+ * (analysis/nonlinear_dynamic.py:602-611).
+ */
+int psx_csr_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values, int value_precision,
+                 const double* x, double alpha, double beta, double* y, void* stream);
+
+/*
  * out[s] = sum of x[i]^2 for offsets[s] <= i < offsets[s+1] (device arrays; offsets int64,
  * n_seg + 1 entries), reduced in a fixed order: the per-mesh residual norms of a batch of
  * meshes stored back to back (the per-instance ||R_free|| test of

@@ -69,6 +69,7 @@ SIGNATURES: dict[str, list] = {
     "psx_fbar_work_doubles": [_i64, _i64, _i64],
     "psx_fbar_element": [_i64, _p, _p, _p, _f64, _f64, _p, _p, _p, _p],
     "psx_ecsw_work_doubles": [_i64, _i32],
+    "psx_csr_spmv": [_i64, _p, _p, _p, _i32, _p, _f64, _f64, _p, _p],
     "psx_ecsw_evaluate": [_i64, _i32, _p, _p, _p, _p, _p, _p, _f64, _f64, _p, _p, _p, _i64, _p, _p],
     "psx_fbar_assemble": [_p, _i64, _i64, _p, _p, _f64, _f64, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p,
                           _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p, _i64, _p, _p],

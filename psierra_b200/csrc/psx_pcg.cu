@@ -458,6 +458,45 @@ extern "C" int psx_csr_dirichlet(int64_t n, const int32_t* indptr, const int32_t
 }
 
 // ---------------------------------------------------------------------------------------
+// y = alpha A x + beta y on a CSR matrix (8 lanes per row, fixed-order lane sums), the
+// products M a and K_0 v of the dynamic residual.
+namespace {
+template <typename VT>
+__global__ void __launch_bounds__(psx::kBlock) csr_spmv_kernel(int64_t n, const int32_t* __restrict__ indptr,
+                                                                const int32_t* __restrict__ indices,
+                                                                const VT* __restrict__ vals,
+                                                                const double* __restrict__ x, double alpha,
+                                                                double beta, double* __restrict__ y) {
+  using namespace psx;
+  const int lane8 = threadIdx.x & (kRowLanes - 1);
+  const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
+  for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
+    const int64_t row = row0 + threadIdx.x / kRowLanes;
+    const double ax = spmv_row<VT>(n, row, lane8, indptr, indices, vals, x);
+    if (row < n && lane8 == 0) y[row] = alpha * ax + (beta != 0.0 ? beta * y[row] : 0.0);
+  }
+}
+}  // namespace
+
+extern "C" int psx_csr_spmv(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                            int value_precision, const double* x, double alpha, double beta, double* y,
+                            void* stream) {
+  using namespace psx;
+  if (n <= 0 || !indptr || !indices || !values || !x || !y) return PSX_ERR_ARG;
+  if (value_precision != PSX_FP64 && value_precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  const int grid = (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (value_precision == PSX_FP64)
+    csr_spmv_kernel<double><<<grid, kBlock, 0, s>>>(n, indptr, indices, static_cast<const double*>(values), x, alpha,
+                                                    beta, y);
+  else
+    csr_spmv_kernel<float><<<grid, kBlock, 0, s>>>(n, indptr, indices, static_cast<const float*>(values), x, alpha,
+                                                   beta, y);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 // Per-segment sums of squares (one block per segment, fixed reduction tree): the residual
 // norms of the meshes of a batch, whose DOFs occupy contiguous ranges of one vector.
 namespace {

@@ -28,7 +28,9 @@ import _refstub  # noqa: E402
 _refstub.install()
 
 from psierra.analysis.dynamic_relaxation import DynamicRelaxationAnalysis  # noqa: E402
+from psierra.analysis.nonlinear_dynamic import NonlinearDynamicAnalysis  # noqa: E402
 from psierra.analysis.nonlinear_static import NonlinearStaticAnalysis  # noqa: E402
+from psierra.damping.rayleigh import RayleighDamping  # noqa: E402
 from psierra.boundary.dirichlet import DirichletConstraint, DirichletManager  # noqa: E402
 from psierra.boundary.load import NodalForce  # noqa: E402
 from psierra.domain.solid import SolidDomain  # noqa: E402
@@ -168,12 +170,29 @@ def fbar_fixture():
                 lam=mat.parameters.lame_parameter_1)
 
 
+def dynamic_fixture():
+    """NonlinearDynamicAnalysis (analysis/nonlinear_dynamic.py) on a small cantilever: tip
+    traction applied at t = 0, generalized-alpha rho_inf = 0.8, Rayleigh damping, the
+    direct linear solver; final u, v, a and the Newton iterations per step."""
+    mb = meshgen.box_tet4(1.0, 0.1, 0.1, 8, 2, 2)
+    mat = nh(1e5, 0.3, rho=1000.0)
+    dm, f_ext, clamp = cantilever_problem(mb, -50.0)
+    dom = SolidDomain(DuckMesh(mb.nodes, mb.elements), mat, Tet4TotalLagrangian(mat))
+    an = NonlinearDynamicAnalysis(dom, damping=RayleighDamping(0.5, 1e-4), spectral_radius=0.8)
+    r = an.solve(dirichlet=dm, f_ext=f_ext, dt=0.05, n_steps=10, nr_iterations=15, nr_tol=1e-8, verbose=False)
+    return dict(u=dom.u.copy(), v=dom.v.copy(), a=dom.a.copy(), iterations=np.array(r.iteration_history),
+                converged=r.converged, f_ext=f_ext, clamp=clamp, dt=0.05, n_steps=10, rho=1000.0,
+                rayleigh=np.array([0.5, 1e-4]), spectral_radius=0.8, nr_tol=1e-8,
+                mu=mat.parameters.shear_modulus, kappa=mat.parameters.bulk_modulus,
+                lam=mat.parameters.lame_parameter_1)
+
+
 def main(only=None):
     rng = np.random.default_rng(20261203)
     out = {}
     if only:
         # fixtures that need no shared random stream can be regenerated on their own
-        gens = {"fbar_box": fbar_fixture}
+        gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture}
         for name in only:
             out[name] = gens[name]()
         for name, d in out.items():
@@ -283,6 +302,7 @@ def main(only=None):
                               converged=r1.converged, f_calls=dom1.f_calls)
 
     out["fbar_box"] = fbar_fixture()
+    out["dynamic_beam"] = dynamic_fixture()
 
     for name, d in out.items():
         path = os.path.join(HERE, f"{name}.npz")
