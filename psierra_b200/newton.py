@@ -97,6 +97,9 @@ class DeviceNewton:
             u = torch.where(self.free, u, lam * up)
             f_step = lam * f_ext
             fnorm = float(torch.linalg.vector_norm(torch.where(self.free, f_step, torch.zeros_like(f_step))))
+            # analysis/nonlinear_static.py:275-331: the step's force scale, or (no load) the
+            # first iteration's max(||R||, ||f_int,free||, 1), kept for the whole step
+            ref = fnorm if fnorm >= 1e-12 else None
             converged = False
             it = 0
             for it in range(1, nr_iterations + 1):
@@ -106,7 +109,9 @@ class DeviceNewton:
                 r = torch.where(self.free, f_step - f, torch.zeros_like(f))
                 rn = float(torch.linalg.vector_norm(r))
                 rhist.append(rn)
-                ref = fnorm if fnorm >= 1e-12 else max(rn, 1.0)
+                if ref is None:
+                    fi = float(torch.linalg.vector_norm(torch.where(self.free, f, torch.zeros_like(f))))
+                    ref = max(rn, fi, 1.0)
                 tol = nr_tol * ref
                 if not np.isfinite(rn):
                     break

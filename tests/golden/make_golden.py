@@ -187,12 +187,30 @@ def dynamic_fixture():
                 lam=mat.parameters.lame_parameter_1)
 
 
+def tet10_newton_fixture():
+    """The Tet10 cube solve at a reduced grid (3^3 cells -> 162 Tet10): clamp z = 0,
+    u_z = -0.2 prescribed on z = 1 and ramped over 8 increments (nonlinear_static.py:
+    271-272), E = 1e4, nu = 0.4, the reference's Newton with its direct solver."""
+    m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, 3, 3, 3))
+    mat = nh(1e4, 0.4)
+    bottom = meshgen.nodes_on_plane(m, 2, "min")
+    top = meshgen.nodes_on_plane(m, 2, "max")
+    dm = DirichletManager(m.n_dofs)
+    dm.add_constraint(DirichletConstraint(bottom, components=(0, 1, 2), value=0.0))
+    dm.add_constraint(DirichletConstraint(top, components=(2,), value=-0.2))
+    dom = SolidDomain(DuckMesh(m.nodes, m.elements), mat, Tet10TotalLagrangian(mat))
+    r = NonlinearStaticAnalysis(dom).solve(dirichlet=dm, f_ext=np.zeros(m.n_dofs), n_steps=8,
+                                           nr_iterations=20, nr_tol=1e-8, verbose=False)
+    return dict(u=r.displacement, converged=r.converged, iterations=np.array(r.iteration_history),
+                bottom=bottom, top=top, mu=mat.parameters.shear_modulus, kappa=mat.parameters.bulk_modulus)
+
+
 def main(only=None):
     rng = np.random.default_rng(20261203)
     out = {}
     if only:
         # fixtures that need no shared random stream can be regenerated on their own
-        gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture}
+        gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture, "tet10_newton": tet10_newton_fixture}
         for name in only:
             out[name] = gens[name]()
         for name, d in out.items():
@@ -303,6 +321,7 @@ def main(only=None):
 
     out["fbar_box"] = fbar_fixture()
     out["dynamic_beam"] = dynamic_fixture()
+    out["tet10_newton"] = tet10_newton_fixture()
 
     for name, d in out.items():
         path = os.path.join(HERE, f"{name}.npz")
