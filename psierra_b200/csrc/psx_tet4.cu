@@ -106,6 +106,12 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
   double Xn[4][3];
   load_nodes(A.X, cn, Xn);
+  // sweeps forming a tangent or K.v load the displacements with the coordinates (one
+  // round trip to memory); the f-only sweep, with fewer registers in use, is faster
+  // loading them after the geometry
+  constexpr bool kEarlyU = !kMass && !kLinear && (kWantK || kKV);
+  double Un[4][3];
+  if constexpr (kEarlyU) load_nodes(A.U, cn, Un);
   Tet4Geom G;
   tet4_geometry(Xn, G);
   if (!(G.detD > 0.0)) flag_bad_element(A.st, e, true);
@@ -142,8 +148,8 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   } else {
     const double mu = A.mu_e ? A.mu_e[e] : A.mu0;
     const double kappa = A.kappa_e ? A.kappa_e[e] : A.kappa0;
-    double Un[4][3], l[3][3];
-    load_nodes(A.U, cn, Un);
+    double l[3][3];
+    if constexpr (!kEarlyU) load_nodes(A.U, cn, Un);
     tet4_grad(Un, G, l);
     PointState ps;
     neohookean_point(l, mu, kappa, ps);
