@@ -154,6 +154,11 @@ typedef struct psx_plan {
   const int32_t* pair_src_t; /* tile * 256 + local pair, ascending tile */
   const int32_t* node_ptr_t; /* N + 1 */
   const int32_t* node_src_t; /* tile * 128 + local node, ascending tile */
+  /* Warp-specialised FP32 tangent sweeps (Tet4; optional, NULL = the mixed kernel): the
+     gather tasks of tasks_k (kinds 1 and 2) in queue order.  With them, f+K and K-only
+     FP32 sweeps run element tiles and gathers in separate warps of one block per SM. */
+  int64_t n_gtasks_k;
+  const int32_t* gtasks_k;  /* device, 4 per task like tasks_k */
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */

@@ -120,6 +120,8 @@ class PlanStruct(ctypes.Structure):
         ("pair_src_t", ctypes.c_void_p),
         ("node_ptr_t", ctypes.c_void_p),
         ("node_src_t", ctypes.c_void_p),
+        ("n_gtasks_k", ctypes.c_int64),
+        ("gtasks_k", ctypes.c_void_p),
     ]
 
 

@@ -95,11 +95,11 @@ class GPUAssembler:
         return 1
 
     def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None,
-                  ring_slack: int | None = None, lag_f: int | None = None) -> None:
+                  ring_slack: int | None = None, lag_f: int | None = None, split: bool | None = None) -> None:
         """Launch shape of the persistent kernel (see ``MeshPattern.set_queue``)."""
         p = self.pattern
         old = (p.lag, p.lag_f, p.ring_slack)
-        p.set_queue(lag=lag, blocks_per_sm=blocks_per_sm, ring_slack=ring_slack, lag_f=lag_f)
+        p.set_queue(lag=lag, blocks_per_sm=blocks_per_sm, ring_slack=ring_slack, lag_f=lag_f, split=split)
         if (p.lag, p.lag_f, p.ring_slack) != old:
             self._work.clear()  # the record ring is sized by the lag and the slack
 

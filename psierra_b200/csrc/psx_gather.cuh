@@ -114,7 +114,7 @@ struct NodeBatch {
 
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list
 // (ascending element) order; their loads are issued kBatch at a time.
-template <typename KT, int NPE, bool TILES = false, bool WANT_F = false>
+template <typename KT, int NPE, bool TILES = false, bool WANT_F = false, int BATCH = 0>
 __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, const KT* __restrict__ krec,
                                             KT* __restrict__ k_out) {
   using L = RecLayout<NPE>;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
   KT acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = (KT)0;
-  constexpr int kBatch = PairBatch<KT, NPE, true, WANT_F>::n;
+  constexpr int kBatch = BATCH > 0 ? BATCH : PairBatch<KT, NPE, true, WANT_F>::n;
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
@@ -167,7 +167,7 @@ struct DRArgs {
 };
 
 // Node item: diagonal block and/or f (or, with DR, the fused pseudo-step on f = K x).
-template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false, bool TILES = false>
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false, bool TILES = false, int BATCH = 0>
 __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, const KT* __restrict__ krec,
                                             const double* __restrict__ frec, KT* __restrict__ k_out,
                                             double* __restrict__ f_out, const DRArgs* dr = nullptr) {
@@ -180,7 +180,7 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc[j] = (KT)0;
   double fa[3] = {0.0, 0.0, 0.0};
-  constexpr int kBatch = NodeBatch<KT, NPE, WANT_K, WANT_F>::n;
+  constexpr int kBatch = BATCH > 0 ? BATCH : NodeBatch<KT, NPE, WANT_K, WANT_F>::n;
   for (int32_t s = s0; s < s1; s += kBatch) {
     int32_t src[kBatch];
 #pragma unroll
@@ -274,7 +274,8 @@ __device__ __forceinline__ void store_diag_block(KT* __restrict__ dst, const KT 
 // ---- persistent task queue --------------------------------------------------------
 // Tasks are claimed by warps (32 elements or 32 items each).  Counters live at the
 // start of the workspace: [0] next task, [1 .. G] element tiles finished per granule,
-// [1 + G .. 2G] gather tiles finished per granule.
+// [1 + G .. 2G] gather tiles finished per granule, [1 + 2G] next gather task of the
+// warp-specialised kernel (whose [0] counts element tiles).
 struct QueueArgs {
   const int4* tasks;
   int32_t n_tasks;
@@ -379,6 +380,80 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
   }
 }
 
+// ---- warp-specialised queue loops -----------------------------------------------------
+// The split kernel runs element tiles and gathers in different warps.  Element tiles are
+// claimed in index order from counter `ecnt` (tile i = elements [i tile, (i+1) tile)),
+// gather tiles in list order from `gcnt` over the gather tasks of the K queue.  The waits
+// are those of drain_queue: an element tile waits for the gathers still reading the ring
+// slots it overwrites, a gather tile for the element tiles of its granule span.  Every
+// task waits only on tasks claimed before it (claims are in order in both lists), so the
+// loops cannot deadlock while the warps that claimed tasks are resident; a wait that
+// gives up flags the status and the task proceeds in bounds.
+template <typename ElementTile>
+__device__ __forceinline__ void drain_elements(const QueueArgs& Q, int32_t* ecnt, Status* st,
+                                               ElementTile&& element_tile) {
+  const int lane = threadIdx.x & 31;
+  int32_t* acnt = Q.counters + 1;
+  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
+  auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  const int64_t n_tiles = (Q.n_elements + Q.tile - 1) / Q.tile;
+  int32_t next = 0;
+  if (lane == 0) next = atomicAdd(ecnt, 1);
+  while (true) {
+    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
+    if (t >= n_tiles) break;
+    if (lane == 0) next = atomicAdd(ecnt, 1);
+    const int64_t e0 = (int64_t)t * Q.tile;
+    const int64_t e1 = min(e0 + (int64_t)Q.tile, Q.n_elements);
+    const int32_t gr = (int32_t)(e0 >> Q.granule_log2);
+    const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
+    if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st);
+    __syncwarp();
+    element_tile(make_int4(0, gr, (int32_t)e0, (int32_t)e1));
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      atomicAdd(acnt + gr, 1);
+    }
+  }
+}
+
+template <typename KT, int NPE, bool WANT_K, bool WANT_F, int PAIR_BATCH, int NODE_BATCH>
+__device__ __forceinline__ void drain_gathers(const GatherArgs& g, const QueueArgs& Q, const int4* __restrict__ gtasks,
+                                              int32_t n_gtasks, int32_t* gcnt, Status* st,
+                                              const KT* __restrict__ krec, const double* __restrict__ frec,
+                                              KT* __restrict__ k_out, double* __restrict__ f_out) {
+  const int lane = threadIdx.x & 31;
+  int32_t* acnt = Q.counters + 1;
+  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
+  const int64_t gsize = (int64_t)1 << Q.granule_log2;
+  auto atiles = [&](int32_t r) -> int32_t {
+    const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
+    return (int32_t)((n + Q.tile - 1) / Q.tile);
+  };
+  int32_t next = 0;
+  if (lane == 0) next = atomicAdd(gcnt, 1);
+  while (true) {
+    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
+    if (t >= n_gtasks) break;
+    if (lane == 0) next = atomicAdd(gcnt, 1);
+    const int4 task = __ldg(gtasks + t);
+    const int32_t gr = task.y;
+    const int32_t first = max(0, gr - Q.span_g - 1);
+    wait_counters(acnt, first, gr - first + 1, atiles, st);
+    __syncwarp();
+    for (int32_t item = task.z + lane; item < task.w; item += 32) {
+      if (task.x == 1) {
+        if constexpr (WANT_K) gather_pair<KT, NPE, true, WANT_F, PAIR_BATCH>(g, item, krec, k_out);
+      } else {
+        gather_node<KT, NPE, WANT_K, WANT_F, false, true, NODE_BATCH>(g, item, krec, frec, k_out, f_out);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) atomicAdd(bcnt + gr, 1);
+  }
+}
+
 inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
   GatherArgs g;
   g.pair_info = P->pair_info;
@@ -480,7 +555,9 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   const int bps = P->blocks_per_sm > 0 ? (P->blocks_per_sm < 4 ? P->blocks_per_sm : 4) : blocks_per_sm;
   W->grid = (int32_t)(sms * bps < ntask ? sms * bps : ntask);
   auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
-  W->counter_bytes = (size_t)up(4 * (1 + 2 * (int64_t)P->n_granules));
+  // [0] next task (next element tile in the split kernel), [1, 1 + G) element tiles done
+  // per granule, [1 + G, 1 + 2G) gather tiles done, [1 + 2G] next gather task (split)
+  W->counter_bytes = (size_t)up(4 * (2 + 2 * (int64_t)P->n_granules));
   int64_t kbytes, fbytes;
   if (W->tiles) {
     const int64_t ring_tiles = W->ring_elems / P->tile;

@@ -595,6 +595,83 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
   drain_queue<KT, 4, S::kWantK, S::kWantF, kDR, S::kTiles>(g, Q, A.st, krec, frec, k_out, f_out, dr, element_tile);
 }
 
+// Warp-specialised FP32 tangent sweep: one block of 16 warps per SM.  Warpgroups 0-1
+// evaluate element tiles and stage them in shared memory (setmaxnreg raises them to
+// kSplitElemRegs registers), warpgroups 2-3 run the gathers (lowered to
+// kSplitGatherRegs).  The gathers' dependent loads then hide behind more warps than the
+// element phase's register need allows in the mixed kernel.  What the gather warps
+// release must cover what the element warps take, so the launch must give each thread
+// exactly kSplitLaunchRegs registers (run_tet4_split checks the compiled kernel).
+#ifndef PSX_SPLIT_PAIR_BATCH
+#define PSX_SPLIT_PAIR_BATCH 4
+#endif
+#ifndef PSX_SPLIT_NODE_BATCH
+#define PSX_SPLIT_NODE_BATCH 1
+#endif
+#ifndef PSX_SPLIT_ELEM_REGS
+#define PSX_SPLIT_ELEM_REGS 168
+#endif
+constexpr int kSplitThreads = 512;
+constexpr int kSplitElemWarps = 8;
+constexpr int kSplitLaunchRegs = 128;
+constexpr int kSplitElemRegs = PSX_SPLIT_ELEM_REGS;
+constexpr int kSplitGatherRegs = 2 * kSplitLaunchRegs - kSplitElemRegs;  // 8 + 8 warps
+static_assert(kSplitThreads * kSplitLaunchRegs == 65536, "one block holds the register file");
+static_assert(kSplitElemWarps * kSplitElemRegs + (kSplitThreads / 32 - kSplitElemWarps) * kSplitGatherRegs ==
+                  (kSplitThreads / 32) * kSplitLaunchRegs,
+              "the register split must add up to the launch allocation");
+static_assert(kSplitElemWarps % 4 == 0, "roles are whole warpgroups");
+
+template <typename KT, int MODE>
+__global__ void __launch_bounds__(kSplitThreads, 1)
+tet4_split_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, const int4* __restrict__ gtasks, int32_t n_gtasks,
+                  KT* __restrict__ krec, double* __restrict__ frec, KT* __restrict__ k_out, double* __restrict__ f_out) {
+  using S = Tet4Smem<KT, MODE>;
+  static_assert(S::kTiles && S::kWantK && sizeof(KT) == 4, "the split kernel runs FP32 tangent sweeps");
+  extern __shared__ __align__(16) unsigned char s_stage[];  // kSplitElemWarps x S::kWarpBytes
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int32_t* ecnt = Q.counters;
+  int32_t* gcnt = Q.counters + 1 + 2 * Q.n_granules;
+  if (warp < kSplitElemWarps) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kSplitElemRegs));
+    unsigned char* my_stage = s_stage + warp * S::kWarpBytes;
+    float* kst = reinterpret_cast<float*>(my_stage);
+    double* fst = reinterpret_cast<double*>(my_stage + sizeof(float) * S::kKFloats);
+    unsigned char* lst = my_stage + sizeof(float) * S::kKFloats + sizeof(double) * S::kFDoubles;
+    drain_elements(Q, ecnt, A.st, [&](const int4& task) {
+      const int64_t t = task.z / g.tile;
+      tile_meta_prefetch(g, t, lst);
+      const int64_t e = task.z + (int64_t)lane;
+      if (e < task.w)
+        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
+                                             fst + kFStride * lane);
+      cp_async_wait_all();
+      __syncwarp();
+      tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
+      __syncwarp();
+    });
+  } else {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kSplitGatherRegs));
+    drain_gathers<KT, 4, S::kWantK, S::kWantF, PSX_SPLIT_PAIR_BATCH, PSX_SPLIT_NODE_BATCH>(
+        g, Q, gtasks, n_gtasks, gcnt, A.st, krec, frec, k_out, f_out);
+  }
+}
+
+// The split kernel is usable when its compiled register count is the one its
+// setmaxnreg split is computed for (checked once per process: the count is a property
+// of the compiled kernel).
+template <typename KT, int MODE>
+bool split_usable() {
+  static int s_regs = -1;
+  if (s_regs < 0) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, tet4_split_kernel<KT, MODE>) != cudaSuccess) return false;
+    s_regs = fa.numRegs;
+  }
+  return s_regs == kSplitLaunchRegs;
+}
+
 __global__ void tet4_dets_kernel(const int32_t* __restrict__ conn, const double* __restrict__ X,
                                  const double* __restrict__ U, int64_t e, double* out2) {
   const int4 cn = reinterpret_cast<const int4*>(conn)[e];
@@ -657,6 +734,47 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   return PSX_OK;
 }
 
+template <typename KT, int MODE>
+int run_tet4_split(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_out, double* f_out,
+                   cudaStream_t stream) {
+  using S = Tet4Smem<KT, MODE>;
+  const GatherArgs g = gather_args(P, W.ring_elems);
+  QueueArgs Q;
+  Q.tasks = reinterpret_cast<const int4*>(P->tasks_k);
+  Q.n_tasks = (int32_t)P->n_tasks_k;
+  Q.n_granules = P->n_granules;
+  Q.btiles = P->btiles_k;
+  Q.counters = W.counters;
+  Q.granule_log2 = W.granule_log2;
+  Q.tile = P->tile;
+  Q.span_g = W.span_g;
+  Q.ring_g = W.ring_g;
+  Q.n_elements = P->n_elements;
+  if (!W.tiles || !S::kTiles || P->tile > 32 || g.tile_k % 4 || g.meta_stride > kMetaBytes) return PSX_ERR_ARG;
+  if (!P->gtasks_k || P->n_gtasks_k <= 0 || P->n_gtasks_k > 0x7fffffff) return PSX_ERR_ARG;
+  if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
+  const size_t smem = kSplitElemWarps * S::kWarpBytes;
+  static unsigned long long s_smem_set = 0;
+  if (set_dynamic_smem_once(tet4_split_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess) return PSX_ERR_CUDA;
+  const int grid = device_sm_count();  // one block (the whole register file) per SM
+  if (grid <= 0) return PSX_ERR_CUDA;
+  tet4_split_kernel<KT, MODE><<<grid, kSplitThreads, smem, stream>>>(
+      A, g, Q, reinterpret_cast<const int4*>(P->gtasks_k), (int32_t)P->n_gtasks_k, static_cast<KT*>(W.krec), W.frec,
+      k_out, f_out);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+// FP32 tangent sweeps take the warp-specialised kernel when the plan carries the gather
+// task list and the kernel's register split is valid; otherwise the mixed kernel.
+template <int MODE>
+int run_tet4_k32(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, float* k_out, double* f_out,
+                 cudaStream_t stream) {
+  if (P->gtasks_k && P->n_gtasks_k > 0 && W.tiles && split_usable<float, MODE>())
+    return run_tet4_split<float, MODE>(P, A, W, k_out, f_out, stream);
+  return run_tet4<float, MODE>(P, A, W, k_out, f_out, stream);
+}
+
 }  // namespace
 }  // namespace psx
 
@@ -698,8 +816,12 @@ extern "C" int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const 
   if (mass) return precision == PSX_FP64 ? PSX_T4(double, PSX_MASS) : PSX_T4(float, PSX_MASS);
   if (linear) return precision == PSX_FP64 ? PSX_T4(double, PSX_LINEAR) : PSX_T4(float, PSX_LINEAR);
   if (wantF && wantK)
-    return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_F | PSX_WANT_K) : PSX_T4(float, PSX_WANT_F | PSX_WANT_K);
-  if (wantK) return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_K) : PSX_T4(float, PSX_WANT_K);
+    return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_F | PSX_WANT_K)
+                                 : run_tet4_k32<PSX_WANT_F | PSX_WANT_K>(plan, A, W, static_cast<float*>(k_out),
+                                                                         f_out, s);
+  if (wantK)
+    return precision == PSX_FP64 ? PSX_T4(double, PSX_WANT_K)
+                                 : run_tet4_k32<PSX_WANT_K>(plan, A, W, static_cast<float*>(k_out), f_out, s);
   return PSX_T4(double, PSX_WANT_F);
 #undef PSX_T4
 }

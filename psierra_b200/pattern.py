@@ -55,6 +55,9 @@ class MeshPattern:
         self._plan_host: dict | None = None
         self.granule, self.tile, self.tile_items, self.lag, self.lag_f, self.ring_slack = self.QUEUE[npe]
         self.blocks_per_sm = 0
+        # Tet4 FP32 tangent sweeps run the warp-specialised kernel (element tiles and
+        # gathers in separate warps) when the plan carries the gather task list
+        self.split = npe == 4
 
     @property
     def n_dofs(self) -> int:
@@ -192,12 +195,26 @@ class MeshPattern:
             setattr(st, "n_tasks_" + key, int(nt.value))
             setattr(st, "tasks_" + key, d["tasks_" + key].data_ptr())
             setattr(st, "btiles_" + key, d["btiles_" + key].data_ptr())
+            if key == "k" and self.npe == 4:
+                # the gather tasks of the K queue in queue order (kinds 1 and 2)
+                tk = tasks[: 4 * int(nt.value)].reshape(-1, 4)
+                gk = np.ascontiguousarray(tk[tk[:, 0] != 0])
+                d["gtasks_k"] = t(gk.reshape(-1) if gk.size else np.zeros(4, dtype=np.int32))
+                d["n_gtasks_k"] = int(gk.shape[0])
+        self._apply_split(d)
+
+    def _apply_split(self, d: dict) -> None:
+        st = d["plan"]
+        on = self.split and d.get("n_gtasks_k", 0) > 0
+        st.n_gtasks_k = d["n_gtasks_k"] if on else 0
+        st.gtasks_k = d["gtasks_k"].data_ptr() if on else None
 
     def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None,
-                  ring_slack: int | None = None, lag_f: int | None = None) -> None:
+                  ring_slack: int | None = None, lag_f: int | None = None, split: bool | None = None) -> None:
         """Change the persistent launch's lags (granules; ``lag`` for the K queue, ``lag_f``
-        for the f / K.v queue), blocks per SM (0 = default) and ring slack (granules beyond
-        span + lag; 0 = the minimum, 6).
+        for the f / K.v queue), blocks per SM (0 = default), ring slack (granules beyond
+        span + lag; 0 = the minimum, 6) and whether Tet4 FP32 tangent sweeps run the
+        warp-specialised kernel (``split``; the mixed kernel otherwise).
 
         Rebuilds the task queues when a lag changes; a workspace sized for the old values
         must be re-queried (``psx_work_bytes``) afterwards.
@@ -214,8 +231,11 @@ class MeshPattern:
             self.blocks_per_sm = int(blocks_per_sm)
         if ring_slack is not None:
             self.ring_slack = int(ring_slack)
+        if split is not None:
+            self.split = bool(split) and self.npe == 4
         if self._dev is not None:
             if rebuild:
                 self._build_tasks(self._dev)
+            self._apply_split(self._dev)
             self._dev["plan"].blocks_per_sm = self.blocks_per_sm
             self._dev["plan"].ring_slack = self.ring_slack
