@@ -177,6 +177,14 @@ int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N, const int3
                   int32_t* node_src, int32_t* node_gptr, int64_t* max_span);
 
 /*
+ * 1 when the warp-specialised Tet4 FP32 tangent kernel can run on the current device
+ * (its compiled register count matches the register split it moves between its element
+ * and gather warps), else 0; FP32 tangent sweeps of a plan with gtasks_k then use the
+ * mixed kernel.  No counterpart in the reference (no GPU path).
+ */
+int psx_tet4_split_ready(void);
+
+/*
  * Tile plan of the Tet4 kernels (host; no counterpart in the reference, which has no
  * element tiles): the element tile of one warp (tile consecutive elements, tile <= 32,
  * a power of two; the plan's `tile`) sums the blocks its elements share in shared

@@ -77,6 +77,7 @@ SIGNATURES: dict[str, list] = {
                                     _p, _i64, _p, _p],
     "psx_tile_plan_fill": [_p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p],
     "psx_tile_meta_stride": [_i32],
+    "psx_tet4_split_ready": [],
 }
 
 

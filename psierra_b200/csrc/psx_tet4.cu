@@ -602,25 +602,44 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
 // element phase's register need allows in the mixed kernel.  What the gather warps
 // release must cover what the element warps take, so the launch must give each thread
 // exactly kSplitLaunchRegs registers (run_tet4_split checks the compiled kernel).
-#ifndef PSX_SPLIT_PAIR_BATCH
-#define PSX_SPLIT_PAIR_BATCH 4
+// Measured alternatives on the 3.07M-element cube (f+K): 12 element + 4 gather warps
+// 1.2-1.4 ms and 4 + 12 1.6 ms (either role starves), 20 or 24 warps per block
+// (fewer registers per role, spills) 0.98-1.09 ms, 8 + 8 at 160-184 element registers
+// within 0.77-0.85 ms.
+// Contributions in flight per gather lane: f+K fastest with 1 pair block, K-only with 2
+// (measured on the 3.07M-element cube: 0.77 vs 0.81 ms, 0.72 vs 0.75 ms).
+#ifndef PSX_SPLIT_PAIR_BATCH_FK
+#define PSX_SPLIT_PAIR_BATCH_FK 1
+#endif
+#ifndef PSX_SPLIT_PAIR_BATCH_K
+#define PSX_SPLIT_PAIR_BATCH_K 2
 #endif
 #ifndef PSX_SPLIT_NODE_BATCH
 #define PSX_SPLIT_NODE_BATCH 1
 #endif
 #ifndef PSX_SPLIT_ELEM_REGS
-#define PSX_SPLIT_ELEM_REGS 168
+#define PSX_SPLIT_ELEM_REGS 176
 #endif
-constexpr int kSplitThreads = 512;
-constexpr int kSplitElemWarps = 8;
-constexpr int kSplitLaunchRegs = 128;
+#ifndef PSX_SPLIT_ELEM_WARPS
+#define PSX_SPLIT_ELEM_WARPS 8
+#endif
+#ifndef PSX_SPLIT_THREADS
+#define PSX_SPLIT_THREADS 512
+#endif
+constexpr int kSplitThreads = PSX_SPLIT_THREADS;
+constexpr int kSplitElemWarps = PSX_SPLIT_ELEM_WARPS;
+constexpr int kSplitLaunchRegs = 65536 / kSplitThreads / 8 * 8;  // what __launch_bounds__(threads, 1) allows
 constexpr int kSplitElemRegs = PSX_SPLIT_ELEM_REGS;
-constexpr int kSplitGatherRegs = 2 * kSplitLaunchRegs - kSplitElemRegs;  // 8 + 8 warps
-static_assert(kSplitThreads * kSplitLaunchRegs == 65536, "one block holds the register file");
-static_assert(kSplitElemWarps * kSplitElemRegs + (kSplitThreads / 32 - kSplitElemWarps) * kSplitGatherRegs ==
+// what the element warps take beyond the launch allocation, the gather warps give up
+constexpr int kSplitGatherRegs =
+    ((kSplitThreads / 32) * kSplitLaunchRegs - kSplitElemWarps * kSplitElemRegs) / (kSplitThreads / 32 - kSplitElemWarps) /
+    8 * 8;
+static_assert(kSplitThreads % 128 == 0 && kSplitThreads * kSplitLaunchRegs <= 65536, "one block per SM, whole warpgroups");
+static_assert(kSplitElemWarps * kSplitElemRegs + (kSplitThreads / 32 - kSplitElemWarps) * kSplitGatherRegs <=
                   (kSplitThreads / 32) * kSplitLaunchRegs,
-              "the register split must add up to the launch allocation");
-static_assert(kSplitElemWarps % 4 == 0, "roles are whole warpgroups");
+              "the register split must fit the launch allocation");
+static_assert(kSplitElemWarps % 4 == 0 && kSplitElemWarps < kSplitThreads / 32, "roles are whole warpgroups");
+static_assert(kSplitElemRegs % 8 == 0 && kSplitElemRegs <= 256 && kSplitGatherRegs >= 24, "setmaxnreg range");
 
 template <typename KT, int MODE>
 __global__ void __launch_bounds__(kSplitThreads, 1)
@@ -653,7 +672,8 @@ tet4_split_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, const int4* __restrict_
     });
   } else {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kSplitGatherRegs));
-    drain_gathers<KT, 4, S::kWantK, S::kWantF, PSX_SPLIT_PAIR_BATCH, PSX_SPLIT_NODE_BATCH>(
+    constexpr int kPairBatch = S::kWantF ? PSX_SPLIT_PAIR_BATCH_FK : PSX_SPLIT_PAIR_BATCH_K;
+    drain_gathers<KT, 4, S::kWantK, S::kWantF, kPairBatch, PSX_SPLIT_NODE_BATCH>(
         g, Q, gtasks, n_gtasks, gcnt, A.st, krec, frec, k_out, f_out);
   }
 }
@@ -779,6 +799,10 @@ int run_tet4_k32(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, fl
 }  // namespace psx
 
 extern "C" size_t psx_status_bytes(void) { return sizeof(psx::Status); }
+
+extern "C" int psx_tet4_split_ready(void) {
+  return psx::split_usable<float, PSX_WANT_F | PSX_WANT_K>() && psx::split_usable<float, PSX_WANT_K>() ? 1 : 0;
+}
 
 extern "C" int psx_work_bytes(const psx_plan_t* plan, int precision, int64_t* ring_elems, int64_t* bytes) {
   // one workspace serves both task queues: the larger of their layouts

@@ -99,13 +99,16 @@ def test_autotuner_keeps_results_bitwise_and_caches(tmp_path):
     f0, k0 = f0.clone(), k0.clone()
     cache = str(tmp_path / "tune.json")
     best = autotune.tune(a, u, lags=(2, 8), blocks=(1, 2), slacks=(6, 16), reps=2, cache_file=cache)
-    assert len(best["table"]) == 8 and best["ms"] > 0
+    # every schedule, mixed or warp-specialised, gives the same bits
+    assert len(best["table"]) == 16 and best["ms"] > 0
     f1, k1 = a.assemble(u)
     assert torch.equal(f0, f1) and torch.equal(k0, k1)
-    for lag, bps, slack in best["table"]:
-        a.set_queue(lag=lag, blocks_per_sm=bps, ring_slack=slack)
+    for lag, bps, slack, split in best["table"]:
+        a.set_queue(lag=lag, blocks_per_sm=bps, ring_slack=slack, split=split)
         f2, k2 = a.assemble(u)
         assert torch.equal(f0, f2) and torch.equal(k0, k2)
+        _, k3 = a.assemble(u, want_f=False)
+        assert torch.equal(k0, k3)
     # the f / K.v queue has its own lag
     y0 = a.kv(u, u).clone()
     for lag_f in (4, 24):
@@ -114,5 +117,5 @@ def test_autotuner_keeps_results_bitwise_and_caches(tmp_path):
     autotune._cache.clear()
     again = autotune.tune(a, u, cache_file=cache)
     assert again["ms"] is None
-    assert (again["lag"], again["blocks_per_sm"], again["ring_slack"]) == (best["lag"], best["blocks_per_sm"],
-                                                                           best["ring_slack"])
+    assert (again["lag"], again["blocks_per_sm"], again["ring_slack"], again["split"]) == (
+        best["lag"], best["blocks_per_sm"], best["ring_slack"], best["split"])

@@ -87,3 +87,65 @@ def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
             srcs = h["node_src"][h["node_ptr"][b]:h["node_ptr"][e]] >> 4
         if srcs.size:
             assert (srcs // granule).min() >= g - span_g - 1 and (srcs // granule).max() <= g
+
+
+@pytest.mark.parametrize("granule,lag,workers,seed", [(128, 0, (1, 1), 0), (128, 2, (3, 2), 1), (256, 4, (2, 5), 2),
+                                                      (64, 0, (4, 4), 3)])
+def test_split_queues_drain(granule, lag, workers, seed):
+    """The warp-specialised kernel's two queues: element tiles claimed in index order by
+    element warps, the gather tasks of the K queue claimed in order by gather warps, with
+    the same waits.  A random schedule of a few workers per role must always drain, and
+    a gather tile may only run once every element tile of its span is done."""
+    m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
+    p = MeshPattern(m.elements, m.n_nodes)
+    p.granule = granule
+    tile = 32
+    tasks, bt, h = _queue(p, 1, tile, lag)
+    G = h["n_granules"]
+    span_g = -(-int(h["max_span"][0]) // granule)
+    all_g = 1 << int(np.ceil(np.log2(max(G, 1))))
+    ring = min(1 << int(np.ceil(np.log2(span_g + lag + 6))), all_g)
+    n_tiles = -(-m.n_elements // tile)
+    gtasks = tasks[tasks[:, 0] != 0]
+    atiles = [-(-min(granule, m.n_elements - r * granule) // tile) for r in range(G)]
+    done_a = np.zeros(G, dtype=np.int64)
+    done_b = np.zeros(G, dtype=np.int64)
+    nxt = {"e": 0, "g": 0}
+    held = {("e", i): None for i in range(workers[0])}
+    held.update({("g", i): None for i in range(workers[1])})
+    rng = np.random.default_rng(seed)
+
+    def ready(role, t):
+        if role == "e":
+            old = t * tile // granule - ring
+            return old < 0 or all(done_b[r] >= bt[r] for r in range(old, min(old + span_g + 2, G)))
+        g = gtasks[t, 1]
+        return all(done_a[r] >= atiles[r] for r in range(max(0, g - span_g - 1), g + 1))
+
+    remaining = n_tiles + len(gtasks)
+    while remaining:
+        moves = []
+        for w, t in held.items():
+            role = w[0]
+            if t is None:
+                if nxt[role] < (n_tiles if role == "e" else len(gtasks)):
+                    moves.append(w)
+            elif ready(role, t):
+                moves.append(w)
+        assert moves, "split queues deadlocked"
+        w = moves[rng.integers(len(moves))]
+        role, t = w[0], held[w]
+        if t is None:
+            held[w] = nxt[role]
+            nxt[role] += 1
+        else:
+            if role == "e":
+                done_a[t * tile // granule] += 1
+            else:
+                g = gtasks[t, 1]
+                # everything this gather tile reads is complete
+                assert all(done_a[r] >= atiles[r] for r in range(max(0, g - span_g - 1), g + 1))
+                done_b[g] += 1
+            held[w] = None
+            remaining -= 1
+    assert (done_a == np.array(atiles)).all() and (done_b == bt).all()
