@@ -289,6 +289,16 @@ struct QueueArgs {
   int64_t n_elements;
 };
 
+// Count one finished element tile: a release add, so the tile's record writes (those
+// of every lane: the caller's __syncwarp orders them before lane 0's release) are
+// visible to a gather that acquires the count.  Used by the warp-specialised kernel
+// (K-only 0.72 -> 0.69 ms on the 3.07M-element cube); the mixed kernel keeps a fence
+// and a plain add, which measured faster there (FP64 K.v 0.36 vs 0.33 ms with the
+// release add).
+__device__ __forceinline__ void publish_tile(int32_t* p) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(p) : "memory");
+}
+
 __device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
   int32_t v;
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -411,10 +421,7 @@ __device__ __forceinline__ void drain_elements(const QueueArgs& Q, int32_t* ecnt
     __syncwarp();
     element_tile(make_int4(0, gr, (int32_t)e0, (int32_t)e1));
     __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      atomicAdd(acnt + gr, 1);
-    }
+    if (lane == 0) publish_tile(acnt + gr);
   }
 }
 
