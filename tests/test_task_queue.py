@@ -149,3 +149,28 @@ def test_split_queues_drain(granule, lag, workers, seed):
             held[w] = None
             remaining -= 1
     assert (done_a == np.array(atiles)).all() and (done_b == bt).all()
+
+
+def test_split_plan_lists_the_gather_tasks_in_queue_order():
+    """The plan's gather-only list (psx_plan_t.gtasks_k) is the K queue without its element
+    tiles, in queue order; switching the split off clears it (the mixed kernel runs)."""
+    m = meshgen.box_tet4(1.0, 1.0, 1.0, 6, 5, 4)
+    p = MeshPattern(m.elements, m.n_nodes)
+    d = p.device("cpu")
+    st = d["plan"]
+    tasks = d["tasks_k"].numpy().reshape(-1, 4)[: st.n_tasks_k]
+    gk = d["gtasks_k"].numpy().reshape(-1, 4)
+    assert np.array_equal(gk, tasks[tasks[:, 0] != 0])
+    assert st.n_gtasks_k == len(gk) and st.gtasks_k == d["gtasks_k"].data_ptr()
+    # element tiles are implicit in the split kernel: consecutive 32-element tiles
+    et = tasks[tasks[:, 0] == 0]
+    assert np.array_equal(et[:, 2], np.arange(len(et)) * p.tile)
+    assert np.array_equal(et[:, 1], et[:, 2] // p.granule)
+    p.set_queue(split=False)
+    assert st.n_gtasks_k == 0 and not st.gtasks_k
+    p.set_queue(split=True)
+    assert st.n_gtasks_k == len(gk) and st.gtasks_k == d["gtasks_k"].data_ptr()
+    # the lag changes the K queue's interleaving, not its gather order
+    p.set_queue(lag=3)
+    d2 = p.device("cpu")
+    assert np.array_equal(d2["gtasks_k"].numpy().reshape(-1, 4), gk)
