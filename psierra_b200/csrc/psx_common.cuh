@@ -146,6 +146,38 @@ __device__ __forceinline__ TangentCoef<T> tangent_coef(const PointState& s, doub
   return t;
 }
 
+// Three consecutive CSR values at p (aligned to the value size) in two streaming stores:
+// the two-value half that is aligned to twice the value size and the remaining value,
+// chosen by predicates so that the lanes of a warp do not diverge.  Each pair block then
+// costs 12 store instructions instead of 18, and fewer partial L2 sector writes.
+__device__ __forceinline__ void store3(float* p, float a, float b, float c) {
+  const bool al = (reinterpret_cast<uintptr_t>(p) & 7) == 0;
+  float2* pv = reinterpret_cast<float2*>(al ? p : p + 1);
+  __stcs(pv, al ? make_float2(a, b) : make_float2(b, c));
+  __stcs(al ? p + 2 : p, al ? c : a);
+}
+
+__device__ __forceinline__ void store3(double* p, double a, double b, double c) {
+  const bool al = (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+  __stcs(reinterpret_cast<double2*>(al ? p : p + 1), al ? make_double2(a, b) : make_double2(b, c));
+  __stcs(al ? p + 2 : p, al ? c : a);
+}
+
+// Add (a, b, c) to three consecutive doubles at p (8-byte aligned), with the same
+// vector + scalar split for the loads and the stores.
+__device__ __forceinline__ void add3(double* p, double a, double b, double c) {
+  const bool al = (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+  double2* pv = reinterpret_cast<double2*>(al ? p : p + 1);
+  double* ps = al ? p + 2 : p;
+  double2 v = *pv;
+  double w = *ps;
+  v.x += al ? a : b;
+  v.y += al ? b : c;
+  w += al ? c : a;
+  *pv = v;
+  *ps = w;
+}
+
 // Status words written by every element kernel (device side).  Counters are
 // reset with a plain memset; `first_bad_key` stores INT32_MAX - e so that an
 // atomicMax picks the lowest element index and a zeroed word means "none".

@@ -323,12 +323,9 @@ __global__ void __launch_bounds__(kFbThreads) fbar_gather(FbarGather G, const do
         for (int j = 0; j < 9; ++j) acc[j] += o[j];
       }
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
+      for (int k = 0; k < 3; ++k) store3(k_out + info[0] + (int64_t)info[1] * k, acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          k_out[info[0] + (int64_t)info[1] * k + m] = acc[3 * k + m];
-          k_out[info[2] + (int64_t)info[3] * m + k] = acc[3 * k + m];
-        }
+      for (int m = 0; m < 3; ++m) store3(k_out + info[2] + (int64_t)info[3] * m, acc[m], acc[3 + m], acc[6 + m]);
     } else {
       const int64_t n = it - G.n_pairs;
       const int32_t* info = G.node_info2 + 4 * n;
@@ -346,13 +343,9 @@ __global__ void __launch_bounds__(kFbThreads) fbar_gather(FbarGather G, const do
         const double full[9] = {d[0], d[1], d[2], d[1], d[3], d[4], d[2], d[4], d[5]};
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) k_out[info[0] + (int64_t)info[1] * k + m] = full[3 * k + m];
+          store3(k_out + info[0] + (int64_t)info[1] * k, full[3 * k], full[3 * k + 1], full[3 * k + 2]);
       }
-      if (f_out) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) f_out[3 * (int64_t)info[2] + k] = f[k];
-      }
+      if (f_out) store3(f_out + 3 * (int64_t)info[2], f[0], f[1], f[2]);
     }
   }
 }
@@ -380,9 +373,7 @@ __global__ void __launch_bounds__(kFbThreads) fbar_vol(int64_t N, const int32_t*
       }
       const int64_t col = 3 * (int64_t)(t - t0);
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int m = 0; m < 3; ++m) k_out[row + stride * k + col + m] += acc[3 * k + m];
+      for (int k = 0; k < 3; ++k) add3(k_out + row + stride * k + col, acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]);
     }
   }
 }

@@ -112,23 +112,6 @@ struct NodeBatch {
   static constexpr int n = sizeof(KT) == 8 ? 2 : (NPE == 4 && WANT_K && WANT_F ? 1 : 4);
 };
 
-// Three consecutive CSR values at p (aligned to the value size) in two streaming stores:
-// the two-value half that is aligned to twice the value size and the remaining value,
-// chosen by predicates so that the lanes of a warp do not diverge.  Each pair block then
-// costs 12 store instructions instead of 18, and fewer partial L2 sector writes.
-__device__ __forceinline__ void store3(float* p, float a, float b, float c) {
-  const bool al = (reinterpret_cast<uintptr_t>(p) & 7) == 0;
-  float2* pv = reinterpret_cast<float2*>(al ? p : p + 1);
-  __stcs(pv, al ? make_float2(a, b) : make_float2(b, c));
-  __stcs(al ? p + 2 : p, al ? c : a);
-}
-
-__device__ __forceinline__ void store3(double* p, double a, double b, double c) {
-  const bool al = (reinterpret_cast<uintptr_t>(p) & 15) == 0;
-  __stcs(reinterpret_cast<double2*>(al ? p : p + 1), al ? make_double2(a, b) : make_double2(b, c));
-  __stcs(al ? p + 2 : p, al ? c : a);
-}
-
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list
 // (ascending element) order; their loads are issued kBatch at a time.
 template <typename KT, int NPE, bool TILES = false, bool WANT_F = false, int BATCH = 0, bool VSTORE = false>
