@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tet10", action="store_true", help="skip the Tet10 assembly measurement")
     ap.add_argument("--no-fbar", action="store_true", help="skip the Tet4Fbar assembly measurement")
+    ap.add_argument("--no-pcg", action="store_true", help="skip the PCG iteration measurement")
     return ap.parse_args()
 
 
@@ -320,11 +321,68 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_kv32, ms_kv64 = (float(x) for x in t.tolist())
 
+    # PCG on the workload's FP32-mixed tangent, clamped at z = 0 (SPD): block-Jacobi,
+    # a fixed number of iterations (rtol = atol = 0).  Time per iteration = difference of
+    # two iteration counts (the set-up and the initial residual cancel).
+    pcg = None
+    if not args.no_pcg:
+        import ctypes
+
+        from psierra_b200 import _lib
+
+        L = _lib.lib()
+        n = 3 * N
+        d = asm.dev
+        kc = k32.clone()
+        fixed = torch.zeros(n, dtype=torch.uint8, device=dev)
+        zfix = np.flatnonzero(np.isclose(m.nodes[:, 2], 0.0))
+        fixed[torch.from_numpy(np.concatenate([3 * zfix + c for c in range(3)])).to(dev)] = 1
+        _lib.check(L.psx_csr_dirichlet(n, _lib.ptr(d["indptr"]), _lib.ptr(d["indices"]), _lib.ptr(kc),
+                                       _lib.PSX_FP32_MIXED, _lib.ptr(fixed),
+                                       torch.cuda.current_stream().cuda_stream), "psx_csr_dirichlet")
+        rhs = torch.from_numpy(np.random.default_rng(11).standard_normal(n)).to(dev)
+        xs = torch.zeros(n, dtype=torch.float64, device=dev)
+        nb = ctypes.c_int64()
+        _lib.check(L.psx_pcg_work_bytes(n, _lib.PSX_PRECOND_BJACOBI, ctypes.byref(nb)), "psx_pcg_work_bytes")
+        pw = torch.empty(int(nb.value), dtype=torch.uint8, device=dev)
+        pst = torch.zeros(16, dtype=torch.int32, device=dev)
+
+        def run_pcg(iters, flags):
+            xs.zero_()
+            pst.zero_()
+            _lib.check(L.psx_pcg_enqueue(n, _lib.ptr(d["indptr"]), _lib.ptr(d["indices"]), _lib.ptr(kc),
+                                         _lib.PSX_FP32_MIXED, _lib.ptr(rhs), _lib.ptr(xs), 0.0, 0.0, iters,
+                                         _lib.PSX_PRECOND_BJACOBI | flags, _lib.ptr(pw), pw.numel(), _lib.ptr(pst),
+                                         torch.cuda.current_stream().cuda_stream), "psx_pcg_enqueue")
+
+        def ms_per_iteration(flags, lo=10, hi=60):
+            ms_lo = time_steps(lambda: run_pcg(lo, flags), max(1, args.steps // 2), args.warmup, sync_all)
+            ms_hi = time_steps(lambda: run_pcg(hi, flags), max(1, args.steps // 2), args.warmup, sync_all)
+            ms = (ms_hi - ms_lo) / (hi - lo)
+            if world > 1:
+                t = torch.tensor([ms], device=dev)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                ms = float(t.item())
+            return ms
+
+        ms_it = ms_per_iteration(_lib.PSX_PCG_NODAL)
+        ms_row = ms_per_iteration(0)
+        # CSR values (fp32) + indices once, ~7 vectors of n doubles (p, q, x, r, z, and the
+        # preconditioner's 3x3 blocks ~ 3 n doubles)
+        bytes_it = 8 * nnz + 8 * 7 * n + 8 * 3 * n
+        pcg = {"workload": "block-Jacobi PCG on the FP32-mixed tangent of the same mesh, clamped at z = 0, "
+                           "fixed iteration count, node-blocked SpMV (PSX_PCG_NODAL)", "ms_per_iteration": ms_it,
+               "algorithmic_bytes_per_iteration": bytes_it, "gbs": bytes_it / (ms_it * 1e-3) / 1e9,
+               "kernels_per_iteration": 3, "row_spmv_ms_per_iteration": ms_row}
+        del kc, pw
+
     # algorithmic bytes per launch (conn 16 E + X,u 48 N + K nnz*s + f 24 N)
     bytes_mixed = 16 * E + 48 * N + 4 * nnz + 24 * N
     bytes_fp64 = 16 * E + 48 * N + 8 * nnz + 24 * N
     bytes_kv = 16 * E + 96 * N
     peak, peak_kind = peak_hbm()
+    if pcg is not None:
+        pcg["frac"] = pcg["gbs"] / peak
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
 
     # Tet10: cube 30^3 Kuhn split upgraded to 10 nodes (162,000 elements, 226,981 nodes,
@@ -447,6 +505,7 @@ def main():
             "accuracy": {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err},
             "tet10": tet10,
             "fbar": fbar,
+            "pcg": pcg,
             "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps * asm.launches_per_call("fp32-mixed"),
             "gpu_launches_note": "assembly timed region; each K.v step is one launch as well",
             "clocks": clk,

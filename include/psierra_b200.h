@@ -375,6 +375,12 @@ int psx_tet4_dr_step(const psx_plan_t* plan, const double* X, const double* u,
 #define PSX_PRECOND_NONE 0
 #define PSX_PRECOND_JACOBI 1     /* 1/diag where |diag| > 1e-14, else 1 (the reference's) */
 #define PSX_PRECOND_BJACOBI 2    /* inverse 3x3 diagonal block per node (n % 3 == 0) */
+/* OR'd into `precond` of the PCG entry points (no counterpart in the reference): the
+   caller guarantees a node-blocked CSR, as psx_csr_pattern builds it -- the three rows of
+   node i have the same columns, in triples 3j, 3j+1, 3j+2 per neighbour j, and row 3i+k
+   starts k * (length of row 3i) after row 3i (n % 3 == 0).  The SpMVs then read each
+   neighbour's columns and x once per node instead of once per row. */
+#define PSX_PCG_NODAL 0x100
 
 /* Workspace bytes of psx_pcg for an n x n system. */
 int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes);

@@ -28,6 +28,7 @@ PSX_FP32_MIXED = 1
 PSX_PRECOND_NONE = 0
 PSX_PRECOND_JACOBI = 1
 PSX_PRECOND_BJACOBI = 2
+PSX_PCG_NODAL = 0x100
 
 _ERRORS = {
     PSX_ERR_ARG: "invalid argument",

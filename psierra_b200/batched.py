@@ -138,8 +138,9 @@ class BatchedNewton:
         self.free = torch.from_numpy((mask == 0).astype(np.float64)).to(dev)
         self.pcg_iterations = int(pcg_iterations)
         self.pcg_rtol = float(pcg_rtol)
+        # the batch's CSR has the assembler's node-blocked layout (PSX_PCG_NODAL)
         self.precond = {"none": _lib.PSX_PRECOND_NONE, "jacobi": _lib.PSX_PRECOND_JACOBI,
-                        "block-jacobi": _lib.PSX_PRECOND_BJACOBI}[preconditioner]
+                        "block-jacobi": _lib.PSX_PRECOND_BJACOBI}[preconditioner] | _lib.PSX_PCG_NODAL
         self.use_graph = use_graph
         f64 = dict(dtype=torch.float64, device=dev)
         B = batch.B

@@ -180,12 +180,62 @@ __device__ __forceinline__ double spmv_row(int64_t n, int64_t row, int lane8, co
   return acc;
 }
 
+// Node-blocked CSR (PSX_PCG_NODAL): the three rows of node i have the same columns, in
+// triples 3j, 3j+1, 3j+2 per neighbour j, and row 3i+k starts k * len after row 3i.  Half
+// a warp per node: lane l takes neighbours l, l + 16, ...; it reads the neighbour's
+// column once (from row 3i), x once for the three rows, and the 3x3 block's values, then
+// the three sums are reduced over the half warp in a fixed order.
+constexpr int kNodeLanes = 16;
+template <typename VT>
+__device__ __forceinline__ void spmv_node(int64_t nodes, int64_t node, int lane16, const int32_t* __restrict__ indptr,
+                                          const int32_t* __restrict__ indices, const VT* __restrict__ vals,
+                                          const double* __restrict__ x, double out[3]) {
+  // nodes past the end run the same shuffles with an empty range
+  int32_t r0 = 0, len = 0;
+  if (node < nodes) {
+    r0 = indptr[3 * node];
+    len = indptr[3 * node + 1] - r0;
+  }
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int32_t b3 = 3 * lane16; b3 < len; b3 += 3 * kNodeLanes) {
+    const int32_t c = indices[r0 + b3];
+    const double x0 = __ldcg(x + c), x1 = __ldcg(x + c + 1), x2 = __ldcg(x + c + 2);
+    const VT* v0 = vals + r0 + b3;
+    const VT* v1 = v0 + len;
+    const VT* v2 = v1 + len;
+    a0 += (double)v0[0] * x0 + (double)v0[1] * x1 + (double)v0[2] * x2;
+    a1 += (double)v1[0] * x0 + (double)v1[1] * x1 + (double)v1[2] * x2;
+    a2 += (double)v2[0] * x0 + (double)v2[1] * x1 + (double)v2[2] * x2;
+  }
+#pragma unroll
+  for (int o = kNodeLanes / 2; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+  }
+  out[0] = a0;
+  out[1] = a1;
+  out[2] = a2;
+}
+
 // r = b - A x, z = M^-1 r, and the sums r.r, r.z, b.b (setup of the iteration).
-template <typename VT, bool BLOCK>
+template <typename VT, bool BLOCK, bool NODAL>
 __global__ void __launch_bounds__(kBlock) pcg_init_residual(int64_t n, const int32_t* __restrict__ indptr,
                                                             const int32_t* __restrict__ indices,
                                                             const VT* __restrict__ vals, const double* __restrict__ b,
                                                             const double* __restrict__ x, PcgWork w) {
+  if constexpr (NODAL) {
+    const int lane16 = threadIdx.x & (kNodeLanes - 1);
+    const int64_t nodes = n / 3, per_pass = (int64_t)gridDim.x * (kBlock / kNodeLanes);
+    for (int64_t node0 = blockIdx.x * (int64_t)(kBlock / kNodeLanes); node0 < nodes; node0 += per_pass) {
+      const int64_t node = node0 + threadIdx.x / kNodeLanes;
+      double ax[3];
+      spmv_node<VT>(nodes, node, lane16, indptr, indices, vals, x, ax);
+      if (node < nodes && lane16 == 0)
+        for (int k = 0; k < 3; ++k) w.r[3 * node + k] = b[3 * node + k] - ax[k];
+    }
+    return;
+  }
   const int lane8 = threadIdx.x & (kRowLanes - 1);
   const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
   for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
@@ -238,20 +288,35 @@ __global__ void __launch_bounds__(kBlock) pcg_update_p(int64_t n, PcgWork w) {
 }
 
 // q = A p and p.q -> alpha = rho / p.q
-template <typename VT>
+template <typename VT, bool NODAL>
 __global__ void __launch_bounds__(kBlock) pcg_spmv(int64_t n, const int32_t* __restrict__ indptr,
                                                    const int32_t* __restrict__ indices, const VT* __restrict__ vals,
                                                    PcgWork w) {
   if (stopped(w.s)) return;
-  const int lane8 = threadIdx.x & (kRowLanes - 1);
   double v[1] = {0.0};
-  const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
-  for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
-    const int64_t row = row0 + threadIdx.x / kRowLanes;
-    const double q = spmv_row<VT>(n, row, lane8, indptr, indices, vals, w.p);
-    if (row < n && lane8 == 0) {
-      w.q[row] = q;
-      v[0] += w.p[row] * q;
+  if constexpr (NODAL) {
+    const int lane16 = threadIdx.x & (kNodeLanes - 1);
+    const int64_t nodes = n / 3, per_pass = (int64_t)gridDim.x * (kBlock / kNodeLanes);
+    for (int64_t node0 = blockIdx.x * (int64_t)(kBlock / kNodeLanes); node0 < nodes; node0 += per_pass) {
+      const int64_t node = node0 + threadIdx.x / kNodeLanes;
+      double q[3];
+      spmv_node<VT>(nodes, node, lane16, indptr, indices, vals, w.p, q);
+      if (node < nodes && lane16 == 0)
+        for (int k = 0; k < 3; ++k) {
+          w.q[3 * node + k] = q[k];
+          v[0] += w.p[3 * node + k] * q[k];
+        }
+    }
+  } else {
+    const int lane8 = threadIdx.x & (kRowLanes - 1);
+    const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
+    for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
+      const int64_t row = row0 + threadIdx.x / kRowLanes;
+      const double q = spmv_row<VT>(n, row, lane8, indptr, indices, vals, w.p);
+      if (row < n && lane8 == 0) {
+        w.q[row] = q;
+        v[0] += w.p[row] * q;
+      }
     }
   }
   double tot[1];
@@ -328,18 +393,19 @@ int layout(int64_t n, int precond, void* work, PcgWork* w, int64_t* bytes) {
   return PSX_OK;
 }
 
-template <typename VT, bool BLOCK>
+template <typename VT, bool BLOCK, bool NODAL>
 int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* vals, const double* b, double* x,
             double rtol, double atol, int32_t maxiter, const PcgWork& w, Status* st, cudaStream_t s,
             int identity, bool host_checks) {
   const int grid_vec = (int)std::min<int64_t>(kGridMax, (n + kBlock - 1) / kBlock);
-  const int grid_row = (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
+  const int grid_row = NODAL ? (int)std::min<int64_t>(kGridMax, (n / 3 + kBlock / kNodeLanes - 1) / (kBlock / kNodeLanes))
+                             : (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
   if (cudaMemsetAsync(w.s, 0, sizeof(PcgScalars), s) != cudaSuccess) return PSX_ERR_CUDA;
   if (BLOCK)
     bjacobi_setup<<<grid_vec, kBlock, 0, s>>>(n / 3, indptr, indices, vals, sizeof(VT) == 4, w.minv, w.s);
   else
     jacobi_setup<<<grid_vec, kBlock, 0, s>>>(n, indptr, indices, vals, sizeof(VT) == 4, w.minv, identity);
-  pcg_init_residual<VT, BLOCK><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, b, x, w);
+  pcg_init_residual<VT, BLOCK, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, b, x, w);
   pcg_init_dots<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, b, w, rtol, atol);
   PSX_CUDA_CHECK_LAUNCH();
   // iterate in batches; every kernel is a no-op once the state is converged or broken down
@@ -350,7 +416,7 @@ int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* 
     const int32_t batch = std::min<int32_t>(kBatchIters, maxiter - done);
     for (int32_t k = 0; k < batch; ++k) {
       pcg_update_p<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, w);
-      pcg_spmv<VT><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, w);
+      pcg_spmv<VT, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, w);
       pcg_update_xr<BLOCK><<<grid_vec, kBlock, 0, s>>>(n, x, w, maxiter);
     }
     PSX_CUDA_CHECK_LAUNCH();
@@ -370,6 +436,7 @@ int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* 
 }  // namespace psx
 
 extern "C" int psx_pcg_work_bytes(int64_t n, int precond, int64_t* bytes) {
+  precond &= ~PSX_PCG_NODAL;
   if (n <= 0 || !bytes || precond < PSX_PRECOND_NONE || precond > PSX_PRECOND_BJACOBI) return PSX_ERR_ARG;
   if (precond == PSX_PRECOND_BJACOBI && n % 3) return PSX_ERR_ARG;
   psx::PcgWork w;
@@ -382,6 +449,9 @@ int pcg_entry(int64_t n, const int32_t* indptr, const int32_t* indices, const vo
               int64_t work_bytes, void* status, void* stream, bool host_checks) {
   using namespace psx;
   if (n <= 0 || !indptr || !indices || !values || !b || !x || !work || !status || maxiter < 0) return PSX_ERR_ARG;
+  const bool nodal = (precond & PSX_PCG_NODAL) != 0;
+  precond &= ~PSX_PCG_NODAL;
+  if (nodal && n % 3) return PSX_ERR_ARG;
   if (precond < PSX_PRECOND_NONE || precond > PSX_PRECOND_BJACOBI) return PSX_ERR_ARG;
   if (precond == PSX_PRECOND_BJACOBI && n % 3) return PSX_ERR_ARG;
   if (value_precision != PSX_FP64 && value_precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
@@ -394,14 +464,16 @@ int pcg_entry(int64_t n, const int32_t* indptr, const int32_t* indices, const vo
   Status* st = static_cast<Status*>(status);
   const bool blk = precond == PSX_PRECOND_BJACOBI;
   const int id = precond == PSX_PRECOND_NONE;
+#define PSX_RUN(VT, BLK, NOD) \
+  run_pcg<VT, BLK, NOD>(n, indptr, indices, static_cast<const VT*>(values), b, x, rtol, atol, maxiter, w, st, s, id, \
+                        host_checks)
   if (value_precision == PSX_FP64) {
-    const double* v = static_cast<const double*>(values);
-    return blk ? run_pcg<double, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks)
-               : run_pcg<double, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks);
+    if (nodal) return blk ? PSX_RUN(double, true, true) : PSX_RUN(double, false, true);
+    return blk ? PSX_RUN(double, true, false) : PSX_RUN(double, false, false);
   }
-  const float* v = static_cast<const float*>(values);
-  return blk ? run_pcg<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks)
-             : run_pcg<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, st, s, id, host_checks);
+  if (nodal) return blk ? PSX_RUN(float, true, true) : PSX_RUN(float, false, true);
+  return blk ? PSX_RUN(float, true, false) : PSX_RUN(float, false, false);
+#undef PSX_RUN
 }
 }  // namespace
 

@@ -105,7 +105,7 @@ class DeviceGeneralizedAlpha:
     def _solve(self, vals: torch.Tensor, rhs: torch.Tensor) -> tuple[torch.Tensor, int]:
         d = self.asm.dev
         x = torch.zeros_like(rhs)
-        res = self.pcg.solve_device(d["indptr"], d["indices"], vals, rhs, x)
+        res = self.pcg.solve_device(d["indptr"], d["indices"], vals, rhs, x, nodal=True)
         if not res.converged:
             raise RuntimeError(f"Conjugate Gradient did not converge (info={res.iterations}).")
         return x, res.iterations

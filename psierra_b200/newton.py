@@ -67,7 +67,7 @@ class DeviceNewton:
         """K x = rhs with the current eliminated tangent; rhs must be zero on fixed DOFs."""
         d = self.asm.dev
         x = torch.zeros_like(rhs)
-        res = self.pcg.solve_device(d["indptr"], d["indices"], self.k, rhs, x)
+        res = self.pcg.solve_device(d["indptr"], d["indices"], self.k, rhs, x, nodal=True)
         if not res.converged:
             raise RuntimeError(f"Conjugate Gradient did not converge (info={res.iterations}).")
         return x, res.iterations

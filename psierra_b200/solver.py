@@ -50,6 +50,32 @@ class PCGResult:
         self.iterations, self.converged, self.residual_norm, self.flags = iterations, converged, residual_norm, flags
 
 
+def is_nodal_csr(indptr, indices) -> bool:
+    """Whether a CSR pattern is node-blocked: the three rows of node i have the same
+    columns, in triples 3j, 3j+1, 3j+2 per neighbour j (the layout ``psx_csr_pattern``
+    builds, and the one ``PSX_PCG_NODAL`` asks for)."""
+    indptr = np.asarray(indptr, dtype=np.int64)
+    indices = np.asarray(indices, dtype=np.int64)
+    n = indptr.size - 1
+    if n <= 0 or n % 3 or indptr[0] != 0 or indices.size < indptr[-1]:
+        return False
+    lens = np.diff(indptr)
+    l3 = lens.reshape(-1, 3)
+    if (lens % 3).any() or not (l3 == l3[:, :1]).all():
+        return False
+    t = indices[: indptr[-1]].reshape(-1, 3)
+    if (t[:, 0] % 3).any() or (t[:, 1] != t[:, 0] + 1).any() or (t[:, 2] != t[:, 0] + 2).any():
+        return False
+    c = t[:, 0]
+    d = l3[:, 0] // 3  # neighbours of each node
+    if d.sum() == 0:
+        return True
+    start = indptr[0:-1:3] // 3  # first triple of row 3i
+    pos = np.repeat(start, d) + (np.arange(d.sum()) - np.repeat(np.cumsum(d) - d, d))
+    dd = np.repeat(d, d)
+    return bool((c[pos + dd] == c[pos]).all() and (c[pos + 2 * dd] == c[pos]).all())
+
+
 class ConjugateGradientSolver(SparseLinearSolver):
     """GPU preconditioned CG with the reference solver's interface and error behaviour."""
 
@@ -74,12 +100,20 @@ class ConjugateGradientSolver(SparseLinearSolver):
         return self._work
 
     def solve_device(self, indptr: torch.Tensor, indices: torch.Tensor, values: torch.Tensor, b: torch.Tensor,
-                     x: torch.Tensor) -> PCGResult:
-        """Solve in place on device tensors (``x`` holds the initial guess on entry)."""
+                     x: torch.Tensor, nodal: bool = False) -> PCGResult:
+        """Solve in place on device tensors (``x`` holds the initial guess on entry).
+
+        ``nodal``: the CSR is node-blocked (``is_nodal_csr``; every matrix of the
+        assembler's pattern is), so the SpMVs read each neighbour's columns once per node.
+        """
         n = b.numel()
         precond = PRECONDITIONERS[self.preconditioner]
         if precond == _lib.PSX_PRECOND_BJACOBI and n % 3:
             raise ValueError("block-jacobi needs a node-aligned system (n % 3 == 0)")
+        if nodal:
+            if n % 3:
+                raise ValueError("a node-blocked system has n % 3 == 0")
+            precond |= _lib.PSX_PCG_NODAL
         vp = _lib.PSX_FP64 if values.dtype == torch.float64 else _lib.PSX_FP32_MIXED
         if values.dtype not in (torch.float64, torch.float32):
             raise ValueError("values must be float64 or float32")
@@ -107,7 +141,7 @@ class ConjugateGradientSolver(SparseLinearSolver):
         values = torch.from_numpy(np.ascontiguousarray(A.data, dtype=np.float64)).to(dev)
         bd = torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).to(dev)
         x = torch.zeros_like(bd)
-        res = self.solve_device(indptr, indices, values, bd, x)
+        res = self.solve_device(indptr, indices, values, bd, x, nodal=is_nodal_csr(A.indptr, A.indices))
         if not res.converged:
             info = self.max_iterations if res.flags == 2 else -1
             raise RuntimeError(f"Conjugate Gradient did not converge (info={info}).")

@@ -168,3 +168,24 @@ def test_fbar_plan_two_ring_and_volumetric_lists():
             for a, qab, qac in entries:
                 assert p.nbr[qab] == b and p.nbr[qac] == c and p.nbr_ptr[a] <= qab < p.nbr_ptr[a + 1]
     assert int(nv.value) == sum(len(r) ** 2 for r in ring1)
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_nodal_csr_layout(name):
+    """The assembler's pattern (and scipy's for the same mesh) is node-blocked, the layout
+    PSX_PCG_NODAL asks for; a free-DOF slice or a reordered row is not."""
+    from psierra_b200.solver import is_nodal_csr
+
+    m = MESHES[name]()
+    p = MeshPattern(m.elements, m.n_nodes)
+    A, _, _ = _scipy_pattern(m.elements, m.n_dofs)
+    assert is_nodal_csr(p.indptr, p.indices)
+    assert is_nodal_csr(A.indptr, A.indices)
+    free = np.arange(1, m.n_dofs)  # one DOF removed
+    S = A[free][:, free].tocsr()
+    assert not is_nodal_csr(S.indptr, S.indices)
+    bad = p.indices.copy()
+    r = int(np.argmax(np.diff(p.indptr) >= 6))  # a row with two neighbours or more
+    a0 = p.indptr[r]
+    bad[a0:a0 + 3], bad[a0 + 3:a0 + 6] = p.indices[a0 + 3:a0 + 6].copy(), p.indices[a0:a0 + 3].copy()
+    assert not is_nodal_csr(p.indptr, bad)
