@@ -148,10 +148,11 @@ def test_tangent_matches_central_differences(precision, tol):
     assert np.allclose(K, K.T, atol=1e-8 * np.abs(K).max())
 
 
-def test_inverted_element_raises_reference_error():
+@pytest.mark.parametrize("precision", ["fp64", "fp32-mixed"])  # fp32-mixed K: the warp-specialised kernel
+def test_inverted_element_raises_reference_error(precision):
     m = meshgen.box_tet4(1.0, 1.0, 1.0, 2, 2, 2)
     u = np.zeros((m.n_nodes, 3))
-    el = Tet4TotalLagrangian(nh(10e3, 0.45))
+    el = Tet4TotalLagrangian(nh(10e3, 0.45), precision=precision)
     f = el.assemble_internal_forces(m, u)
     assert np.abs(f).max() < 1e-12
     # push node 0 of element 7 through the opposite face
@@ -170,8 +171,11 @@ def test_inverted_element_raises_reference_error():
     with pytest.raises(ValueError, match="Element inversion detected") as ei:
         el.assemble_internal_forces(m, u)
     assert f"{Jref:.4e}" in str(ei.value)
-    with pytest.raises(ValueError, match="Element inversion detected"):
+    with pytest.raises(ValueError, match="Element inversion detected") as ei:
         el.assemble_tangent_stiffness_matrix(m, u)
+    assert f"{Jref:.4e}" in str(ei.value)
+    with pytest.raises(ValueError, match="Element inversion detected"):
+        el.assemble_force_and_tangent(m, u)
 
 
 def test_negative_volume_raises_reference_error():
