@@ -38,15 +38,19 @@ struct GatherArgs {
   int32_t p0, p1;            // pair item range of this launch
   int32_t n0, n1;            // node item range of this launch
   int64_t ring_mask;
-  // tile records (Tet4): lists name (tile, local pair / node); a tile's ring slot holds
-  // cap_p pair blocks (12 values), cap_n diagonal blocks (8 values) and cap_n f triples
+  // tile records (Tet4): lists name (tile, local pair / node).  A tile's ring slot holds,
+  // with cap_p4 / cap_n4 = cap_p / cap_n rounded up to a multiple of 4, the planes
+  // P0 (cap_p4 float4: pair values 0-3), P1 (float4: 4-7), P2 (cap_p4 floats: value 8),
+  // D0 (cap_n4 float4: xx xy xz yy), D1 (cap_n4 float2: yz zz) in the K ring and
+  // F0, F1, F2 (cap_n4 doubles: f x, y, z) in the f ring
   const int32_t* pair_ptr_t;
   const int32_t* pair_src_t;  // tile * 256 + local pair
   const int32_t* node_ptr_t;
   const int32_t* node_src_t;  // tile * 128 + local node
   int64_t ring_tile_mask;
   int32_t cap_p, cap_n;
-  int32_t tile_k;             // K values per tile record: 12 cap_p + 8 cap_n
+  int32_t cap_p4, cap_n4;
+  int32_t tile_k;             // K values per tile record: 9 cap_p4 + 6 cap_n4
   // per-tile reduction lists (psx_tile_plan_fill): one block of meta_stride bytes per
   // tile, fields at byte offsets off_p (pair offsets), off_n (node offsets), src_p (pair
   // codes), src_n (node codes); byte 0 / 1 = pair / node count
@@ -134,10 +138,16 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (src[b] >= 0) {
-        if constexpr (TILES)
-          load_block<KT, 12>(krec + ((int64_t)(src[b] >> 8) & g.ring_tile_mask) * g.tile_k + 12 * (src[b] & 255),
-                             v[b]);
-        else
+        if constexpr (TILES) {
+          // pair planes of the tile record (K is FP32 wherever tile records hold K)
+          const float* base = reinterpret_cast<const float*>(krec) + ((int64_t)(src[b] >> 8) & g.ring_tile_mask) * g.tile_k;
+          const int lp = src[b] & 255;
+          const float4 x = __ldcg(reinterpret_cast<const float4*>(base) + lp);
+          const float4 y = __ldcg(reinterpret_cast<const float4*>(base + 4 * g.cap_p4) + lp);
+          v[b][0] = x.x; v[b][1] = x.y; v[b][2] = x.z; v[b][3] = x.w;
+          v[b][4] = y.x; v[b][5] = y.y; v[b][6] = y.z; v[b][7] = y.w;
+          v[b][8] = __ldcg(base + 8 * g.cap_p4 + lp);
+        } else
           load_block<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * L::kK + L::pair_off(src[b] & 63), v[b]);
       }
 #pragma unroll
@@ -198,24 +208,34 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (src[b] >= 0) {
-        const KT* kp;
-        const double* fp;
         if constexpr (TILES) {
+          // diagonal and f planes of the tile record (K is FP32 wherever it is present)
           const int64_t slot = (int64_t)(src[b] >> 7) & g.ring_tile_mask;
           const int ln = src[b] & 127;
-          kp = krec + slot * g.tile_k + 12 * g.cap_p + 8 * ln;
-          fp = frec + slot * 3 * g.cap_n + 3 * ln;
+          if constexpr (WANT_K) {
+            const float* base = reinterpret_cast<const float*>(krec) + slot * g.tile_k + 9 * g.cap_p4;
+            const float4 x = __ldcg(reinterpret_cast<const float4*>(base) + ln);
+            const float2 y = __ldcg(reinterpret_cast<const float2*>(base + 4 * g.cap_n4) + ln);
+            v[b][0] = x.x; v[b][1] = x.y; v[b][2] = x.z; v[b][3] = x.w;
+            v[b][4] = y.x; v[b][5] = y.y;
+          }
+          if constexpr (WANT_F) {
+            const double* fb = frec + slot * 3 * g.cap_n4 + ln;
+            fv[b][0] = __ldcg(fb);
+            fv[b][1] = __ldcg(fb + g.cap_n4);
+            fv[b][2] = __ldcg(fb + 2 * g.cap_n4);
+          }
         } else {
           const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;
           const int a = src[b] & 15;
-          kp = krec + slot * L::kK + L::diag_off(a);
-          fp = frec + slot * L::kF + 3 * a;
-        }
-        if constexpr (WANT_K) load_block<KT, 8>(kp, v[b]);
-        if constexpr (WANT_F) {
-          fv[b][0] = __ldcg(fp);
-          fv[b][1] = __ldcg(fp + 1);
-          fv[b][2] = __ldcg(fp + 2);
+          const KT* kp = krec + slot * L::kK + L::diag_off(a);
+          const double* fp = frec + slot * L::kF + 3 * a;
+          if constexpr (WANT_K) load_block<KT, 8>(kp, v[b]);
+          if constexpr (WANT_F) {
+            fv[b][0] = __ldcg(fp);
+            fv[b][1] = __ldcg(fp + 1);
+            fv[b][2] = __ldcg(fp + 2);
+          }
         }
       }
 #pragma unroll
@@ -496,7 +516,9 @@ inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
   g.node_src_t = P->node_src_t;
   g.cap_p = P->tile_cap_pairs;
   g.cap_n = P->tile_cap_nodes;
-  g.tile_k = 12 * g.cap_p + 8 * g.cap_n;
+  g.cap_p4 = (g.cap_p + 3) / 4 * 4;  // every plane starts on a 16-byte boundary
+  g.cap_n4 = (g.cap_n + 3) / 4 * 4;
+  g.tile_k = 9 * g.cap_p4 + 6 * g.cap_n4;
   g.tile_meta = P->tile_meta;
   g.tile = P->tile;
   {
@@ -587,8 +609,10 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
   int64_t kbytes, fbytes;
   if (W->tiles) {
     const int64_t ring_tiles = W->ring_elems / P->tile;
-    kbytes = queue_k ? up(ring_tiles * (12 * (int64_t)P->tile_cap_pairs + 8 * (int64_t)P->tile_cap_nodes) * kt) : 0;
-    fbytes = up(ring_tiles * 3 * (int64_t)P->tile_cap_nodes * 8);
+    // planar tile records (GatherArgs): 9 cap_p4 + 6 cap_n4 K values, 3 cap_n4 f doubles
+    const int64_t cp4 = (P->tile_cap_pairs + 3) / 4 * 4, cn4 = (P->tile_cap_nodes + 3) / 4 * 4;
+    kbytes = queue_k ? up(ring_tiles * (9 * cp4 + 6 * cn4) * kt) : 0;
+    fbytes = up(ring_tiles * 3 * cn4 * 8);
   } else {
     kbytes = queue_k ? up(W->ring_elems * kK * kt) : 0;
     fbytes = up(W->ring_elems * kF * 8);

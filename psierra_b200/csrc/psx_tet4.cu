@@ -483,7 +483,10 @@ __device__ __forceinline__ void tile_meta_prefetch(const GatherArgs& g, int64_t 
 }
 
 // Sum the staged element blocks of tile `t` into its tile record (one warp), with the
-// tile's lists in shared memory (`lst`, tile_meta_prefetch).
+// tile's lists in shared memory (`lst`, tile_meta_prefetch).  The record is stored in
+// planes (gather_args): pair values 0-3, 4-7 and 8, diagonal xx xy xz yy and yz zz, and
+// f x, y, z, each plane contiguous over the tile's pairs or nodes, so that every store
+// of the warp writes whole sectors.
 template <bool WANT_K, bool WANT_F>
 __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, const unsigned char* __restrict__ lst,
                                             const float* __restrict__ kst, const double* __restrict__ fst,
@@ -491,45 +494,51 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
   using L = RecLayout<4>;
   const int lane = threadIdx.x & 31;
   const int64_t slot = t & g.ring_tile_mask;
+  float* kbase = krec + slot * g.tile_k;
   if constexpr (WANT_K) {
     const int np = lst[0];
     const unsigned char* off = lst + g.off_p;
     const unsigned char* src = lst + g.src_p;
-    float4* rec = reinterpret_cast<float4*>(krec + slot * g.tile_k);
+    float4* p0 = reinterpret_cast<float4*>(kbase);
+    float4* p1 = reinterpret_cast<float4*>(kbase + 4 * g.cap_p4);
+    float* p2 = kbase + 8 * g.cap_p4;
     for (int lp = lane; lp < np; lp += 32) {
       const int a0 = off[lp], a1 = off[lp + 1];
-      float4 s[3] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
-                     make_float4(0.f, 0.f, 0.f, 0.f)};
+      float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+      float s2 = 0.f;
       for (int q = a0; q < a1; ++q) {
         const int c = src[q];
-        const float4* b = reinterpret_cast<const float4*>(kst + (c >> 3) * kStageStride + L::pair_off(c & 7));
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          const float4 x = b[r];
-          s[r].x += x.x; s[r].y += x.y; s[r].z += x.z; s[r].w += x.w;
-        }
+        const float* b = kst + (c >> 3) * kStageStride + L::pair_off(c & 7);
+        const float4 x = reinterpret_cast<const float4*>(b)[0], y = reinterpret_cast<const float4*>(b)[1];
+        s0.x += x.x; s0.y += x.y; s0.z += x.z; s0.w += x.w;
+        s1.x += y.x; s1.y += y.y; s1.z += y.z; s1.w += y.w;
+        s2 += b[8];
       }
-#pragma unroll
-      for (int r = 0; r < 3; ++r) __stcg(rec + 3 * lp + r, s[r]);
+      __stcg(p0 + lp, s0);
+      __stcg(p1 + lp, s1);
+      __stcg(p2 + lp, s2);
     }
   }
   const int nn = lst[1];
   const unsigned char* off = lst + g.off_n;
   const unsigned char* src = lst + g.src_n;
-  float4* drec = reinterpret_cast<float4*>(krec + slot * g.tile_k + 12 * g.cap_p);
-  double* frow = frec + slot * 3 * g.cap_n;
+  float4* d0p = reinterpret_cast<float4*>(kbase + 9 * g.cap_p4);
+  float2* d1p = reinterpret_cast<float2*>(kbase + 9 * g.cap_p4 + 4 * g.cap_n4);
+  double* fb = frec + slot * 3 * g.cap_n4;
   for (int ln = lane; ln < nn; ln += 32) {
     const int a0 = off[ln], a1 = off[ln + 1];
-    float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f), d1 = d0;
+    float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 d1 = make_float2(0.f, 0.f);
     double f0 = 0.0, f1 = 0.0, f2 = 0.0;
     for (int q = a0; q < a1; ++q) {
       const int c = src[q];
       const int el = c >> 2, a = c & 3;
       if constexpr (WANT_K) {
         const float4* b = reinterpret_cast<const float4*>(kst + el * kStageStride + L::diag_off(a));
-        const float4 x = b[0], y = b[1];
+        const float4 x = b[0];
+        const float2 y = reinterpret_cast<const float2*>(b + 1)[0];
         d0.x += x.x; d0.y += x.y; d0.z += x.z; d0.w += x.w;
-        d1.x += y.x; d1.y += y.y; d1.z += y.z; d1.w += y.w;
+        d1.x += y.x; d1.y += y.y;
       }
       if constexpr (WANT_F) {
         const double* fp = fst + el * kFStride + 3 * a;
@@ -539,13 +548,13 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
       }
     }
     if constexpr (WANT_K) {
-      __stcg(drec + 2 * ln, d0);
-      __stcg(drec + 2 * ln + 1, d1);
+      __stcg(d0p + ln, d0);
+      __stcg(d1p + ln, d1);
     }
     if constexpr (WANT_F) {
-      __stcg(frow + 3 * ln, f0);
-      __stcg(frow + 3 * ln + 1, f1);
-      __stcg(frow + 3 * ln + 2, f2);
+      __stcg(fb + ln, f0);
+      __stcg(fb + g.cap_n4 + ln, f1);
+      __stcg(fb + 2 * g.cap_n4 + ln, f2);
     }
   }
 }
