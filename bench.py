@@ -231,7 +231,7 @@ def main():
         m, u, mat = make_problem(args.cells)
         vals = []
         for i in range(args.warmup + args.steps):
-            cb = cpu_baseline(m, u, mat, max(2000, args.cpu_sample // 4))
+            cb = cpu_baseline(m, u, mat, args.cpu_sample)  # the sample size of the other arm's baseline
             if i >= args.warmup:
                 vals.append(cb["value"])
         v = float(np.median(vals))
