@@ -10,7 +10,7 @@ from conftest import golden, rel_2, rel_max
 from oracle.assembly import assemble_mass
 from psierra_b200 import meshgen
 from psierra_b200.analysis import DynamicRelaxationAnalysis, NonlinearStaticAnalysis
-from psierra_b200.domain import DirichletConstraint, DirichletManager, NodalForce, SolidDomain
+from psierra_b200.domain import DirichletConstraint, DirichletManager, SolidDomain
 from psierra_b200.element import Tet4TotalLagrangian
 from psierra_b200.material import IsotropicElasticParameters, NeoHookean
 from psierra_b200.solver import ConjugateGradientSolver

@@ -7,7 +7,6 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
-import torch
 
 from oracle.tet4 import force_and_tangent
 from psierra_b200 import meshgen

@@ -8,7 +8,6 @@ from __future__ import annotations
 import numpy as np
 import pytest
 import scipy.sparse as spsp
-import torch
 
 from conftest import golden
 from oracle import tet4fbar
