@@ -104,6 +104,39 @@ __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
   }
 }
 
+// Tet4 element records in the global ring are stored in planes: the 16-byte granule i of
+// the record of ring slot s lies at krec + (i * plane + s) * W (W = 16 / sizeof(KT) values,
+// plane = ring length), so that the 32 lanes of a warp, which write consecutive slots,
+// write whole sectors.  `base` = krec + s * W; `o` = value offset inside the record
+// (RecLayout<4>, a multiple of W).
+template <typename KT, int N>
+__device__ __forceinline__ void store_planes(KT* __restrict__ base, int o, const KT v[N], int64_t plane) {
+  constexpr int W = 16 / (int)sizeof(KT);
+#pragma unroll
+  for (int i = 0; i < N / W; ++i) {
+    KT* q = base + (int64_t)(o / W + i) * plane * W;
+    if constexpr (W == 4)
+      __stcg(reinterpret_cast<float4*>(q), make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+    else
+      __stcg(reinterpret_cast<double2*>(q), make_double2(v[2 * i], v[2 * i + 1]));
+  }
+}
+template <typename KT, int N>
+__device__ __forceinline__ void load_planes(const KT* __restrict__ base, int o, KT v[N], int64_t plane) {
+  constexpr int W = 16 / (int)sizeof(KT);
+#pragma unroll
+  for (int i = 0; i < N / W; ++i) {
+    const KT* q = base + (int64_t)(o / W + i) * plane * W;
+    if constexpr (W == 4) {
+      const float4 t = __ldcg(reinterpret_cast<const float4*>(q));
+      v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+    } else {
+      const double2 t = __ldcg(reinterpret_cast<const double2*>(q));
+      v[2 * i] = t.x; v[2 * i + 1] = t.y;
+    }
+  }
+}
+
 // Contributions whose loads are issued together, kept within the register budget: the
 // fused FP32 f + K Tet4 kernel runs 3 blocks per SM, which its 168 registers allow only
 // with two pair and one node contribution in flight; the other sweeps keep four.
@@ -147,8 +180,13 @@ __device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, cons
           v[b][0] = x.x; v[b][1] = x.y; v[b][2] = x.z; v[b][3] = x.w;
           v[b][4] = y.x; v[b][5] = y.y; v[b][6] = y.z; v[b][7] = y.w;
           v[b][8] = __ldcg(base + 8 * g.cap_p4 + lp);
-        } else
+        } else if constexpr (NPE == 4) {
+          constexpr int W = 16 / (int)sizeof(KT);
+          load_planes<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * W, L::pair_off(src[b] & 63), v[b],
+                              g.ring_mask + 1);
+        } else {
           load_block<KT, 12>(krec + ((int64_t)(src[b] >> 6) & g.ring_mask) * L::kK + L::pair_off(src[b] & 63), v[b]);
+        }
       }
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
@@ -224,6 +262,20 @@ __device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, cons
             fv[b][0] = __ldcg(fb);
             fv[b][1] = __ldcg(fb + g.cap_n4);
             fv[b][2] = __ldcg(fb + 2 * g.cap_n4);
+          }
+        } else if constexpr (NPE == 4) {
+          // planar Tet4 element records (store_planes); f: value j of the 12 at granule j/2
+          constexpr int W = 16 / (int)sizeof(KT);
+          const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;
+          const int64_t plane = g.ring_mask + 1;
+          const int a = src[b] & 15;
+          if constexpr (WANT_K) load_planes<KT, 8>(krec + slot * W, L::diag_off(a), v[b], plane);
+          if constexpr (WANT_F) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const int vj = 3 * a + j;
+              fv[b][j] = __ldcg(frec + slot * 2 + (int64_t)(vj >> 1) * plane * 2 + (vj & 1));
+            }
           }
         } else {
           const int64_t slot = (int64_t)(src[b] >> 4) & g.ring_mask;

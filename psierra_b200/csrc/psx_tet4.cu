@@ -72,6 +72,8 @@ struct Tet4Args {
   // of density rho, K_0 the small-strain stiffness (lam0, mu0, or per element
   // lambda = kappa_e - 2/3 mu_e, mu_e)
   double c_t, c_m, c_0, rho;
+  // element records in the global ring (store_planes): the ring length (set by run_tet4)
+  int64_t plane = 0;
 };
 
 // Phase A: one element -> its record.  tet4_total_lagrangian.py:77-139 (and, with
@@ -81,15 +83,39 @@ struct Tet4Args {
 // 12 f / y doubles of an element: an L2-only store to the global ring, or plain stores to
 // the shared-memory staging of the element tile.
 template <bool FGLOBAL>
-__device__ __forceinline__ void store_f12(double* __restrict__ frec, const double v[12]) {
+__device__ __forceinline__ void store_f12(double* __restrict__ frec, const double v[12], int64_t plane = 0) {
   if constexpr (FGLOBAL) {
-    double2* fq = reinterpret_cast<double2*>(frec);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) __stcg(fq + i, make_double2(v[2 * i], v[2 * i + 1]));
+    store_planes<double, 12>(frec, 0, v, plane);  // frec = ring + 2 * slot
   } else {
     double2* fq = reinterpret_cast<double2*>(frec);
 #pragma unroll
     for (int i = 0; i < 6; ++i) fq[i] = make_double2(v[2 * i], v[2 * i + 1]);
+  }
+}
+
+// A block of the element's record: planes of the global ring (KGLOBAL: krec = ring +
+// W * slot), or the lane's shared-memory staging (krec = the staged record).
+template <typename KT, bool KGLOBAL>
+__device__ __forceinline__ void put_pair(KT* __restrict__ krec, int o, const KT b[9], bool swap, int64_t plane) {
+  if constexpr (KGLOBAL) {
+    KT v[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) v[3 * k + m] = swap ? b[3 * m + k] : b[3 * k + m];
+    v[9] = v[10] = v[11] = (KT)0;
+    store_planes<KT, 12>(krec, o, v, plane);
+  } else {
+    store_pair_block<KT, false>(krec + o, b, swap);
+  }
+}
+template <typename KT, bool KGLOBAL>
+__device__ __forceinline__ void put_diag(KT* __restrict__ krec, int o, const KT d[6], int64_t plane) {
+  if constexpr (KGLOBAL) {
+    const KT v[8] = {d[0], d[1], d[2], d[3], d[4], d[5], (KT)0, (KT)0};
+    store_planes<KT, 8>(krec, o, v, plane);
+  } else {
+    store_diag_block<KT, false>(krec + o, d);
   }
 }
 
@@ -121,9 +147,9 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     const KT off[9] = {mm, 0, 0, 0, mm, 0, 0, 0, mm};
     const KT d[6] = {(KT)2 * mm, 0, 0, (KT)2 * mm, 0, (KT)2 * mm};
 #pragma unroll
-    for (int slot = 0; slot < 6; ++slot) store_pair_block<KT, KGLOBAL>(krec + L::pair_off(slot), off, false);
+    for (int slot = 0; slot < 6; ++slot) put_pair<KT, KGLOBAL>(krec, L::pair_off(slot), off, false, A.plane);
 #pragma unroll
-    for (int a = 0; a < 4; ++a) store_diag_block<KT, KGLOBAL>(krec + L::diag_off(a), d);
+    for (int a = 0; a < 4; ++a) put_diag<KT, KGLOBAL>(krec, L::diag_off(a), d, A.plane);
     return;
   }
   KT p[4][3], q[4][3];
@@ -177,7 +203,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 #pragma unroll
         for (int i = 0; i < 3; ++i)
           fr[3 * a + i] = G.V * (ps.P[i][0] * G.g[a][0] + ps.P[i][1] * G.g[a][1] + ps.P[i][2] * G.g[a][2]);
-      store_f12<FGLOBAL>(frec, fr);
+      store_f12<FGLOBAL>(frec, fr, A.plane);
     }
     if constexpr (kWantK || kKV) {
       tc = tangent_coef<KT>(ps, kappa, G.V);
@@ -427,9 +453,9 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
           }
         if (b == a) {
           const KT d[6] = {v[0], v[1], v[2], v[4], v[5], v[8]};
-          store_diag_block<KT, KGLOBAL>(krec + L::diag_off(a), d);
+          put_diag<KT, KGLOBAL>(krec, L::diag_off(a), d, A.plane);
         } else {
-          store_pair_block<KT, KGLOBAL>(krec + L::pair_off(slot), v, gid[a] > gid[b]);
+          put_pair<KT, KGLOBAL>(krec, L::pair_off(slot), v, gid[a] > gid[b], A.plane);
           ++slot;
         }
       }
@@ -597,7 +623,7 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
     } else {
       for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
         const int64_t slot = e & g.ring_mask;
-        tet4_element<KT, MODE>(A, e, krec + slot * L::kK, frec + slot * L::kF);
+        tet4_element<KT, MODE>(A, e, krec + slot * (16 / (int64_t)sizeof(KT)), frec + slot * 2);  // planar records
       }
     }
   };
@@ -762,7 +788,9 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
     grid = (int)(want < ntask ? want : ntask);
     if (grid <= 0) grid = 1;
   }
-  tet4_persistent_kernel<KT, MODE><<<grid, kThreads, smem, stream>>>(A, g, Q, static_cast<KT*>(W.krec), W.frec,
+  Tet4Args Ap = A;
+  Ap.plane = W.ring_elems;  // element records are stored in planes of the ring (store_planes)
+  tet4_persistent_kernel<KT, MODE><<<grid, kThreads, smem, stream>>>(Ap, g, Q, static_cast<KT*>(W.krec), W.frec,
                                                                     k_out, f_out, dr);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
