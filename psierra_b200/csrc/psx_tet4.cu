@@ -637,17 +637,16 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
 // element phase's register need allows in the mixed kernel.  What the gather warps
 // release must cover what the element warps take, so the launch must give each thread
 // exactly kSplitLaunchRegs registers (run_tet4_split checks the compiled kernel).
-// Measured alternatives on the 3.07M-element cube (f+K): 12 element + 4 gather warps
-// 1.2-1.4 ms and 4 + 12 1.6 ms (either role starves), 20 or 24 warps per block
-// (fewer registers per role, spills) 0.98-1.09 ms, 8 + 8 at 160-184 element registers
-// within 0.77-0.85 ms.
-// Contributions in flight per gather lane: 2 pair blocks for f+K and K-only (with the
-// planar tile records, on the 3.07M-element cube: f+K 0.672 ms against 0.694 with 1 and
-// 0.687 with 2 pair and 2 node blocks).  The sweeps
-// without a tangent (f, K.v, DR step) stay on the mixed kernel: their FP64 element
-// phase is the bottleneck and their node gathers are light, so giving half the warps
-// to gathers doubled their time (K.v 0.30 -> 0.58 ms with 8 + 8 warps, 0.93 ms with
-// 4 + 12).
+//
+// Measured on the 3.07M-element cube (f+K):
+// * roles: 12 element + 4 gather warps 1.2-1.4 ms and 4 + 12 1.6 ms (either role
+//   starves), 20 or 24 warps per block (fewer registers per role, spills) 0.98-1.09 ms,
+//   8 + 8 with 160-184 element registers within 2-4 % of each other;
+// * contributions in flight per gather lane: 2 pair blocks (0.672 ms against 0.694 with
+//   1, and 0.687 with 2 pair and 2 node blocks, with the planar tile records);
+// * the sweeps without a tangent (f, K.v, DR step) stay on the mixed kernel: their FP64
+//   element phase is the bottleneck and their node gathers are light, so giving half
+//   the warps to gathers doubled their time (K.v 0.30 -> 0.58 ms with 8 + 8 warps).
 #ifndef PSX_SPLIT_PAIR_BATCH_FK
 #define PSX_SPLIT_PAIR_BATCH_FK 2
 #endif
