@@ -350,31 +350,43 @@ __global__ void __launch_bounds__(kFbThreads) fbar_gather(FbarGather G, const do
   }
 }
 
-// two-ring block (b, c): K += sum_a (kappa v0_a) (g_a[b] g_a[c]^T), a ascending
+// two-ring block (b, c): K += sum_a (kappa v0_a) (g_a[b] g_a[c]^T), a ascending.  One
+// thread per two-ring entry t (the block of node b and its t-th two-ring neighbour; b
+// found by a binary search of nbr2_ptr), so that the threads of a warp update adjacent
+// blocks of the same rows.
 __global__ void __launch_bounds__(kFbThreads) fbar_vol(int64_t N, const int32_t* __restrict__ nbr2_ptr,
                                                        const int32_t* __restrict__ vol_ptr,
                                                        const int32_t* __restrict__ vol_src,
                                                        const double* __restrict__ v0, const double* __restrict__ g,
                                                        double kappa, double* __restrict__ k_out) {
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < N; b += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t n2 = nbr2_ptr[N];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += (int64_t)gridDim.x * blockDim.x) {
+    // the node b with nbr2_ptr[b] <= t < nbr2_ptr[b + 1]
+    int64_t lo = 0, hi = N;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) / 2;
+      if (nbr2_ptr[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int64_t b = lo;
     const int32_t t0 = nbr2_ptr[b], t1 = nbr2_ptr[b + 1];
     const int64_t row = 9 * (int64_t)t0, stride = 3 * (int64_t)(t1 - t0);
-    for (int32_t t = t0; t < t1; ++t) {
-      double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int32_t s = vol_ptr[t]; s < vol_ptr[t + 1]; ++s) {
-        const int32_t* v = vol_src + 3 * (int64_t)s;
-        const double sc = kappa * v0[v[0]];
-        const double* gb = g + 3 * (int64_t)v[1];
-        const double* gc = g + 3 * (int64_t)v[2];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int32_t s = vol_ptr[t]; s < vol_ptr[t + 1]; ++s) {
+      const int32_t* v = vol_src + 3 * (int64_t)s;
+      const double sc = kappa * v0[v[0]];
+      const double* gb = g + 3 * (int64_t)v[1];
+      const double* gc = g + 3 * (int64_t)v[2];
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+      for (int k = 0; k < 3; ++k)
 #pragma unroll
-          for (int m = 0; m < 3; ++m) acc[3 * k + m] += sc * (gb[k] * gc[m]);
-      }
-      const int64_t col = 3 * (int64_t)(t - t0);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) add3(k_out + row + stride * k + col, acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]);
+        for (int m = 0; m < 3; ++m) acc[3 * k + m] += sc * (gb[k] * gc[m]);
     }
+    const int64_t col = 3 * (t - t0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) add3(k_out + row + stride * k + col, acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]);
   }
 }
 
@@ -532,7 +544,8 @@ extern "C" int psx_fbar_assemble(const int32_t* conn, int64_t E, int64_t N, cons
   if (k_out && cudaMemsetAsync(k_out, 0, sizeof(double) * nnz2, s) != cudaSuccess) return PSX_ERR_CUDA;
   FbarGather G{pair_info2, pair_ptr, pair_src, node_info2, node_ptr, node_src, n_pairs, N};
   fbar_gather<<<fb_grid(n_pairs + N), kFbThreads, 0, s>>>(G, A.rec, k_out, f_out);
-  if (k_out) fbar_vol<<<fb_grid(N), kFbThreads, 0, s>>>(N, nbr2_ptr, vol_ptr, vol_src, A.v0, A.g, kappa, k_out);
+  // one thread per two-ring entry: the two-ring CSR holds 9 values per entry
+  if (k_out) fbar_vol<<<fb_grid(nnz2 / 9), kFbThreads, 0, s>>>(N, nbr2_ptr, vol_ptr, vol_src, A.v0, A.g, kappa, k_out);
   PSX_CUDA_CHECK_LAUNCH();
   return PSX_OK;
 }
