@@ -137,25 +137,34 @@ __global__ void __launch_bounds__(kFbThreads) fbar_nodes(FbarArgs A) {
 }
 
 // g_a[b] for every one-ring entry (a, b): thread per node a
+// One thread per one-ring entry t (node a and its neighbour; a found by a binary search
+// of nbr_ptr), so that a warp writes consecutive entries.
 __global__ void __launch_bounds__(kFbThreads) fbar_patch(FbarArgs A) {
-  for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.N; a += (int64_t)gridDim.x * blockDim.x) {
-    const double v0 = A.v0[a];
-    for (int32_t t = A.nbr_ptr[a]; t < A.nbr_ptr[a + 1]; ++t) {
-      double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-      for (int32_t s = A.blk_ptr[t]; s < A.blk_ptr[t + 1]; ++s) {
-        const int32_t code = A.blk_src[s];
-        const int32_t lb = code & 3;
-        const int64_t e = code >> 4;
-        const double w = 0.25 * A.V[e] * A.J[e] / v0;
-        const double* qe = A.q + 12 * e + 3 * lb;
-        g0 += w * qe[0];
-        g1 += w * qe[1];
-        g2 += w * qe[2];
-      }
-      A.g[3 * (int64_t)t] = g0;
-      A.g[3 * (int64_t)t + 1] = g1;
-      A.g[3 * (int64_t)t + 2] = g2;
+  const int64_t n1 = A.nbr_ptr[A.N];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n1; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = A.N;  // nbr_ptr[lo] <= t < nbr_ptr[hi]
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) / 2;
+      if (A.nbr_ptr[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
     }
+    const double v0 = A.v0[lo];
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    for (int32_t s = A.blk_ptr[t]; s < A.blk_ptr[t + 1]; ++s) {
+      const int32_t code = A.blk_src[s];
+      const int32_t lb = code & 3;
+      const int64_t e = code >> 4;
+      const double w = 0.25 * A.V[e] * A.J[e] / v0;
+      const double* qe = A.q + 12 * e + 3 * lb;
+      g0 += w * qe[0];
+      g1 += w * qe[1];
+      g2 += w * qe[2];
+    }
+    A.g[3 * t] = g0;
+    A.g[3 * t + 1] = g1;
+    A.g[3 * t + 2] = g2;
   }
 }
 
@@ -539,7 +548,7 @@ extern "C" int psx_fbar_assemble(const int32_t* conn, int64_t E, int64_t N, cons
   A.E = E; A.N = N;
   fbar_pre<<<fb_grid(E), kFbThreads, 0, s>>>(A);
   fbar_nodes<<<fb_grid(N), kFbThreads, 0, s>>>(A);
-  if (k_out) fbar_patch<<<fb_grid(N), kFbThreads, 0, s>>>(A);
+  if (k_out) fbar_patch<<<fb_grid(n_nbr), kFbThreads, 0, s>>>(A);  // one thread per one-ring entry
   fbar_element<<<fb_grid(E), kFbThreads, 0, s>>>(A);
   if (k_out && cudaMemsetAsync(k_out, 0, sizeof(double) * nnz2, s) != cudaSuccess) return PSX_ERR_CUDA;
   FbarGather G{pair_info2, pair_ptr, pair_src, node_info2, node_ptr, node_src, n_pairs, N};
