@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-tet10", action="store_true", help="skip the Tet10 assembly measurement")
     ap.add_argument("--no-fbar", action="store_true", help="skip the Tet4Fbar assembly measurement")
     ap.add_argument("--no-pcg", action="store_true", help="skip the PCG iteration measurement")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the accuracy check against the oracle")
+    ap.add_argument("--oracle-nodes", type=int, default=2000, help="nodes whose rows the oracle checks")
     return ap.parse_args()
 
 
@@ -127,6 +129,30 @@ def cpu_baseline(m, u, mat, sample: int):
                    f"(assemble_internal_forces + assemble_tangent_stiffness_matrix) split over {len(jobs)} "
                    f"processes ({t_loop:.2f} s), then COO->CSR + np.add.at in one process ({t_asm:.2f} s)"),
     }
+
+
+def oracle_rows_check(m, u, mat, asm, k64, f64, k32, f32, count: int = 2000, seed: int = 17):
+    """Accuracy of both GPU results against the oracle (the checker, outside any timed
+    region): the rows of ``count`` seeded nodes, which the elements incident to them give
+    exactly (``oracle.sample``)."""
+    from oracle import sample as osample
+
+    t0 = time.perf_counter()
+    nodes = osample.sample_nodes(m.n_nodes, count, seed)
+    dofs, K_ref, f_ref = osample.sampled_rows(m.nodes, m.elements, u, mat.parameters.shear_modulus,
+                                              mat.parameters.bulk_modulus, nodes)
+    out = {}
+    ip, ix = asm.pattern.indptr, asm.pattern.indices
+    for tag, k, f in (("fp64", k64, f64), ("mixed", k32, f32)):
+        same, err = osample.compare_rows(osample.gpu_rows(ip, ix, k.double().cpu().numpy(), dofs), K_ref)
+        fd = f.cpu().numpy()[dofs]
+        out[f"K_{tag}_vs_oracle_max_rel"] = err
+        out[f"f_{tag}_vs_oracle_rel2"] = float(np.linalg.norm(fd - f_ref) / np.linalg.norm(f_ref))
+        out[f"pattern_{tag}_equal_oracle"] = bool(same)
+    out["oracle_sample"] = (f"rows of {nodes.size} seeded nodes ({dofs.size} DOFs, {K_ref.nnz} K values): "
+                            f"the oracle evaluates the elements incident to them and sums them by COO->CSR "
+                            f"({time.perf_counter() - t0:.1f} s)")
+    return out
 
 
 # --------------------------------------------------------------------------- clocks
@@ -283,6 +309,9 @@ def main():
     asm.assemble(u_dev, precision="fp32-mixed", f_out=f32, k_out=k32)
     k_err = float(((k32.double() - k64).abs().max() / k64.abs().max()).item())
     f_err = float(((f32 - f64).norm() / f64.norm()).item())
+    accuracy = {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err}
+    if rank == 0 and not args.no_oracle:
+        accuracy.update(oracle_rows_check(m, u, mat, asm, k64, f64, k32, f32, count=args.oracle_nodes))
 
     def step_mixed():
         asm.assemble(u_dev, precision="fp32-mixed", f_out=f32, k_out=k32, check_status=False)
@@ -502,7 +531,7 @@ def main():
                             "frac": bytes_kv / (ms_kv64 * 1e-3) / 1e9 / peak,
                             "elements_per_s": world * E / (ms_kv64 * 1e-3)},
                    "mixed_vs_fp64_rel2": kv_err},
-            "accuracy": {"K_mixed_vs_fp64_max_rel": k_err, "f_mixed_vs_fp64_rel2": f_err},
+            "accuracy": accuracy,
             "tet10": tet10,
             "fbar": fbar,
             "pcg": pcg,

@@ -159,6 +159,12 @@ typedef struct psx_plan {
      FP32 sweeps run element tiles and gathers in separate warps of one block per SM. */
   int64_t n_gtasks_k;
   const int32_t* gtasks_k;  /* device, 4 per task like tasks_k */
+  /* Polls of one bounded wait of the persistent kernels before it gives up (status flag
+     bit 0, which the host turns into an error; every later wait of the launch then
+     returns at once).  0 = the default, 1 << 22 polls (about a second).  A small value
+     lets a test make a wait run out without faulting the GPU. */
+  int32_t wait_spins;
+  int32_t reserved0;        /* 0 */
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */
@@ -443,8 +449,16 @@ int psx_csr_dirichlet(int64_t n, const int32_t* indptr, const int32_t* indices, 
  * GPU that loads it until the process exits (psx_pcg_static_max_bytes() returns the
  * size).  It allocates nothing.  Systems whose psx_pcg_work_bytes exceeds the scratch
  * are rejected with PSX_ERR_LIMIT: about n <= 838,000 unknowns with the Jacobi
- * preconditioner and n <= 599,000 with block-Jacobi.  The first call on a device looks up
- * the scratch address on that device; make that first call before any stream capture.
+ * preconditioner and n <= 599,000 with block-Jacobi.  The array is reserved when the CUDA
+ * runtime loads this library's CG module on a device: at context creation when the
+ * process runs with CUDA_MODULE_LOADING=EAGER, otherwise (lazy loading, the CUDA 12
+ * default) at the first call that uses the module on that device, which a
+ * psx_pcg_static call does.  A caller that must have all its device memory reserved
+ * before its run either sets CUDA_MODULE_LOADING=EAGER or makes one psx_pcg_static call
+ * on each device during its set-up; later calls reserve nothing more.  The first call on
+ * a device also looks up the scratch address on that device; make that first call before
+ * any stream capture.  Like psx_pcg, the solve reads its convergence test back to the
+ * host every 16 iterations (a device-to-host copy and a synchronisation of `stream`).
  * Every call on a device shares the one array, so calls that overlap on the GPU (other
  * streams, other host threads) race; the scalars the solve needs at zero are cleared at
  * the start of every call.  Arguments and results are those of psx_pcg.

@@ -124,6 +124,8 @@ class PlanStruct(ctypes.Structure):
         ("node_src_t", ctypes.c_void_p),
         ("n_gtasks_k", ctypes.c_int64),
         ("gtasks_k", ctypes.c_void_p),
+        ("wait_spins", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
     ]
 
 

@@ -32,6 +32,16 @@ def _stream_handle() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+WAIT_GAVE_UP = 1  # status flag bit 0: a bounded wait of a persistent kernel gave up
+
+
+def raise_if_wait_gave_up(flags: int) -> None:
+    """Raise when status ``flags`` say a bounded wait gave up: the kernel ran to its end,
+    but records may have been read before they were written, so its outputs are invalid."""
+    if int(flags) & WAIT_GAVE_UP:
+        raise RuntimeError("psierra_b200: a bounded wait in the assembly kernel gave up; results are invalid")
+
+
 class GPUAssembler:
     """Assembler for one Tet4 or Tet10 mesh with a NeoHookean material (constant or per element)."""
 
@@ -102,6 +112,11 @@ class GPUAssembler:
         p.set_queue(lag=lag, blocks_per_sm=blocks_per_sm, ring_slack=ring_slack, lag_f=lag_f, split=split)
         if (p.lag, p.lag_f, p.ring_slack) != old:
             self._work.clear()  # the record ring is sized by the lag and the slack
+
+    def set_wait_limit(self, spins: int) -> None:
+        """Polls after which a bounded wait of the persistent kernels gives up (0 = the
+        default, about a second); see ``MeshPattern.set_wait_limit``."""
+        self.pattern.set_wait_limit(spins)
 
     def workspace(self, precision: str) -> torch.Tensor:
         w = self._work.get(precision)
@@ -232,17 +247,27 @@ class GPUAssembler:
 
     def dr_step(self, u: torch.Tensor, b: torch.Tensor, minv: torch.Tensor, x: torch.Tensor, vel: torch.Tensor,
                 c1: float, c2: float, dt: float, precision: str | None = None,
-                r_out: torch.Tensor | None = None) -> None:
-        """One fused dynamic-relaxation pseudo-step on ``K_T(u) x = b`` (updates x, vel in place)."""
+                r_out: torch.Tensor | None = None, check_status: bool = True) -> None:
+        """One fused dynamic-relaxation pseudo-step on ``K_T(u) x = b`` (updates x, vel in place).
+
+        With ``check_status`` (the default) the sweep's status is read afterwards, which
+        synchronises: an inverted element raises the reference's ``ValueError`` and a
+        bounded wait that gave up raises ``RuntimeError``.  Loops that check less often
+        pass ``check_status=False`` and call ``raise_on_bad_elements`` themselves; the
+        status is zeroed before every step either way.
+        """
         prec = precision or self.precision
         u = self._check_u(u)
         for t in (b, minv, x, vel):
             self._check_u(t)
+        self.status.zero_()
         work = self.workspace(prec)
         check(lib().psx_tet4_dr_step(ctypes.byref(self.dev["plan"]), ptr(self.X), ptr(u), ptr(self.mu_e),
                                      ptr(self.kappa_e), self.mu, self.kappa, PRECISIONS[prec], ptr(b), ptr(minv),
                                      c1, c2, dt, ptr(x), ptr(vel), ptr(r_out), ptr(work), work.numel(),
                                      ptr(self.status), _stream_handle()), "psx_tet4_dr_step")
+        if check_status:
+            self.raise_on_bad_elements(u)
 
     def _check_u(self, u: torch.Tensor) -> torch.Tensor:
         if not isinstance(u, torch.Tensor) or u.device != self.X.device or u.dtype != torch.float64:
@@ -264,8 +289,7 @@ class GPUAssembler:
 
     def raise_on_bad_elements(self, u: torch.Tensor | None) -> None:
         n_inv, n_vol, first, flags = self.status_counts()
-        if flags & 1:
-            raise RuntimeError("psierra_b200: a bounded wait in the assembly kernel gave up; results are invalid")
+        raise_if_wait_gave_up(flags)
         if n_inv == 0 and n_vol == 0:
             return
         if self.npe == 10:

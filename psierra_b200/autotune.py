@@ -19,6 +19,8 @@ import os
 
 import torch
 
+from psierra_b200.assembler import raise_if_wait_gave_up
+
 DEFAULT_LAGS = (8, 12, 16, 24)
 DEFAULT_BLOCKS = (2,)
 DEFAULT_SLACKS = (6, 12, 20)
@@ -43,6 +45,9 @@ def _time(asm, u, precision, want_f, want_k, f, k, reps: int) -> float:
         asm.assemble(u, want_f=want_f, want_k=want_k, precision=precision, f_out=f, k_out=k, check_status=False)
     b.record()
     b.synchronize()
+    # the status of the last timed call: a candidate whose bounded wait gave up is not a
+    # valid launch shape
+    raise_if_wait_gave_up(asm.status_counts()[3])
     return a.elapsed_time(b) / reps
 
 

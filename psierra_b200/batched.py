@@ -36,7 +36,7 @@ import torch
 
 from psierra_b200 import _lib
 from psierra_b200._lib import check, lib, ptr
-from psierra_b200.assembler import GPUAssembler
+from psierra_b200.assembler import GPUAssembler, raise_if_wait_gave_up
 from psierra_b200.material import NeoHookeanField
 from psierra_b200.meshgen import concat_meshes
 
@@ -247,6 +247,9 @@ class BatchedNewton:
                 # an inverted element makes its instance's residual non-finite (ln J of
                 # J <= 0), which retires that instance below
                 rn2 = self.rn2.cpu().numpy()
+                # the replay assembled with check_status=False: a bounded wait that gave
+                # up leaves a K_T summed out of order, so no instance may use this step
+                raise_if_wait_gave_up(self.asm.status_counts()[3])
                 hist.append(np.sqrt(rn2))
                 newly = alive & ~conv & (rn2 < tol * tol)  # the device's test, negated
                 its[step - 1, newly] = it

@@ -56,35 +56,24 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = True, out: str | None = None, defines=()) -> str:
-    """Compile every CUDA/C++ source and link the shared library; returns its path.
-
-    ``out``/``defines`` build a variant (e.g. another register budget) under another name.
-    """
-    global BUILD
-    lib = out or LIB
-    if out is None and not defines and not force and not _stale():
+def build(force: bool = False, verbose: bool = True) -> str:
+    """Compile every CUDA/C++ source and link the shared library; returns its path."""
+    if not force and not _stale():
         return LIB
-    if defines:
-        BUILD = os.path.join(ROOT, "_build", "variant_" + "_".join(d.replace("=", "") for d in defines))
-        CUDA_FLAGS.extend(f"-D{d}" for d in defines)
     os.makedirs(BUILD, exist_ok=True)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(_compile, srcs))
-    tmp = lib + ".tmp"
+    tmp = LIB + ".tmp"
     cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, lib)
+    os.replace(tmp, LIB)
     if verbose:
-        print(f"built {lib}")
-    return lib
+        print(f"built {LIB}")
+    return LIB
 
 
 if __name__ == "__main__":
-    args = [a for a in sys.argv[1:] if a != "--force"]
-    defs = [a[2:] for a in args if a.startswith("-D")]
-    outs = [a[6:] for a in args if a.startswith("--out=")]
-    build(force="--force" in sys.argv, out=outs[0] if outs else None, defines=defs)
+    build(force="--force" in sys.argv)

@@ -373,7 +373,10 @@ struct QueueArgs {
   int32_t span_g;         // max item span in granules (rounded up)
   int32_t ring_g;         // ring length in granules (power of two)
   int64_t n_elements;
+  int32_t max_spins;      // polls of one bounded wait before it gives up
 };
+
+constexpr int32_t kDefaultWaitSpins = 1 << 22;  // about a second with the 200 ns back-off
 
 // Count one finished element tile: a release add, so the tile's record writes (those
 // of every lane: the caller's __syncwarp orders them before lane 0's release) are
@@ -397,9 +400,8 @@ __device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
 // host reports the failure.
 template <typename Target>
 __device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first, int32_t count, Target target,
-                                              Status* st) {
+                                              Status* st, int32_t max_spins) {
   const int lane = threadIdx.x & 31;
-  constexpr int kMaxSpins = 1 << 22;
   for (int32_t base = 0; base < count; base += 32) {
     const int32_t g = first + base + lane;
     const bool mine = (base + lane) < count && g >= 0;
@@ -409,7 +411,7 @@ __device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first,
       const bool ok = !mine || ld_acquire(cnt + g) >= want;
       if (__all_sync(0xffffffffu, ok)) break;
       // once any wait has given up, every later wait returns at once
-      if (++spins > kMaxSpins || (ld_acquire(&st->flags) & 1)) {
+      if (++spins > max_spins || (ld_acquire(&st->flags) & 1)) {
         if (lane == 0) atomicOr(&st->flags, 1);
         return false;
       }
@@ -451,7 +453,7 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
     const int32_t gr = task.y;
     if (task.x == 0) {
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st);
+      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st, Q.max_spins);
       __syncwarp();
       element_tile(task);
       __syncwarp();
@@ -461,7 +463,7 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
       }
     } else {
       const int32_t first = max(0, gr - Q.span_g - 1);
-      wait_counters(acnt, first, gr - first + 1, atiles, st);
+      wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
       __syncwarp();
       for (int32_t item = task.z + lane; item < task.w; item += 32) {
         // K row segments leave as vector + scalar pairs (FP64 f+K 2.35 -> 2.26 ms, Tet10
@@ -505,7 +507,7 @@ __device__ __forceinline__ void drain_elements(const QueueArgs& Q, int32_t* ecnt
     const int64_t e1 = min(e0 + (int64_t)Q.tile, Q.n_elements);
     const int32_t gr = (int32_t)(e0 >> Q.granule_log2);
     const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-    if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st);
+    if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st, Q.max_spins);
     __syncwarp();
     element_tile(make_int4(0, gr, (int32_t)e0, (int32_t)e1));
     __syncwarp();
@@ -535,7 +537,7 @@ __device__ __forceinline__ void drain_gathers(const GatherArgs& g, const QueueAr
     const int4 task = __ldg(gtasks + t);
     const int32_t gr = task.y;
     const int32_t first = max(0, gr - Q.span_g - 1);
-    wait_counters(acnt, first, gr - first + 1, atiles, st);
+    wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
     __syncwarp();
     // K values leave in float2 + float pairs per row segment: 12 instead of 18 store
     // instructions per pair block (f+K 0.76 -> 0.72 ms, K-only 0.69 -> 0.64 ms on the
@@ -681,6 +683,24 @@ inline int work_layout(const psx_plan_t* P, int precision, void* work, WorkLayou
     W->frec = reinterpret_cast<double*>(w + W->counter_bytes + kbytes);
   }
   return PSX_OK;
+}
+
+// Queue arguments of one launch: the K queue (sweeps with pair gathers) or the f / K.v
+// queue, on the workspace layout W.
+inline QueueArgs queue_args(const psx_plan_t* P, const WorkLayout& W, bool queue_k) {
+  QueueArgs Q;
+  Q.tasks = reinterpret_cast<const int4*>(queue_k ? P->tasks_k : P->tasks_f);
+  Q.n_tasks = (int32_t)(queue_k ? P->n_tasks_k : P->n_tasks_f);
+  Q.n_granules = P->n_granules;
+  Q.btiles = queue_k ? P->btiles_k : P->btiles_f;
+  Q.counters = W.counters;
+  Q.granule_log2 = W.granule_log2;
+  Q.tile = P->tile;
+  Q.span_g = W.span_g;
+  Q.ring_g = W.ring_g;
+  Q.n_elements = P->n_elements;
+  Q.max_spins = P->wait_spins > 0 ? P->wait_spins : kDefaultWaitSpins;
+  return Q;
 }
 
 }  // namespace psx

@@ -309,17 +309,7 @@ int run_tet10(const psx_plan_t* P, const Tet10Args& A, const WorkLayout& W, KT* 
               cudaStream_t stream) {
   constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
   const GatherArgs g = gather_args(P, W.ring_elems);
-  QueueArgs Q;
-  Q.tasks = reinterpret_cast<const int4*>(kWantK ? P->tasks_k : P->tasks_f);
-  Q.n_tasks = (int32_t)(kWantK ? P->n_tasks_k : P->n_tasks_f);
-  Q.n_granules = P->n_granules;
-  Q.btiles = kWantK ? P->btiles_k : P->btiles_f;
-  Q.counters = W.counters;
-  Q.granule_log2 = W.granule_log2;
-  Q.tile = P->tile;
-  Q.span_g = W.span_g;
-  Q.ring_g = W.ring_g;
-  Q.n_elements = P->n_elements;
+  const QueueArgs Q = queue_args(P, W, kWantK);
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
   const size_t smem = sizeof(Tet10Smem<KT>) * (kThreads10 / 32);
   static unsigned long long s_smem_set = 0;

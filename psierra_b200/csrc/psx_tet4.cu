@@ -758,17 +758,7 @@ int run_tet4(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, KT* k_
   constexpr bool kWantK =
       (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0 && (MODE & (PSX_KV | kModeAdjoint)) == 0;
   const GatherArgs g = gather_args(P, W.ring_elems);
-  QueueArgs Q;
-  Q.tasks = reinterpret_cast<const int4*>(kWantK ? P->tasks_k : P->tasks_f);
-  Q.n_tasks = (int32_t)(kWantK ? P->n_tasks_k : P->n_tasks_f);
-  Q.n_granules = P->n_granules;
-  Q.btiles = kWantK ? P->btiles_k : P->btiles_f;
-  Q.counters = W.counters;
-  Q.granule_log2 = W.granule_log2;
-  Q.tile = P->tile;
-  Q.span_g = W.span_g;
-  Q.ring_g = W.ring_g;
-  Q.n_elements = P->n_elements;
+  const QueueArgs Q = queue_args(P, W, kWantK);
   using S = Tet4Smem<KT, MODE>;
   // the kernel's record format (tile or element records) must be the one the workspace
   // was laid out for
@@ -800,17 +790,7 @@ int run_tet4_split(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, 
                    cudaStream_t stream) {
   using S = Tet4Smem<KT, MODE>;
   const GatherArgs g = gather_args(P, W.ring_elems);
-  QueueArgs Q;
-  Q.tasks = reinterpret_cast<const int4*>(P->tasks_k);
-  Q.n_tasks = (int32_t)P->n_tasks_k;
-  Q.n_granules = P->n_granules;
-  Q.btiles = P->btiles_k;
-  Q.counters = W.counters;
-  Q.granule_log2 = W.granule_log2;
-  Q.tile = P->tile;
-  Q.span_g = W.span_g;
-  Q.ring_g = W.ring_g;
-  Q.n_elements = P->n_elements;
+  const QueueArgs Q = queue_args(P, W, true);
   if (!W.tiles || !S::kTiles || P->tile > 32 || g.tile_k % 4 || g.meta_stride > kMetaBytes) return PSX_ERR_ARG;
   if (!P->gtasks_k || P->n_gtasks_k <= 0 || P->n_gtasks_k > 0x7fffffff) return PSX_ERR_ARG;
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;

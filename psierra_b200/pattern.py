@@ -55,6 +55,7 @@ class MeshPattern:
         self._plan_host: dict | None = None
         self.granule, self.tile, self.tile_items, self.lag, self.lag_f, self.ring_slack = self.QUEUE[npe]
         self.blocks_per_sm = 0
+        self.wait_spins = 0  # polls of one bounded wait in the persistent kernels (0 = about a second)
         # Tet4 FP32 tangent sweeps run the warp-specialised kernel (element tiles and
         # gathers in separate warps) when the plan carries the gather task list
         self.split = npe == 4
@@ -182,6 +183,7 @@ class MeshPattern:
         st.tile, st.lag, st.lag_f, st.tile_items = self.tile, self.lag, self.lag_f, self.tile_items
         st.blocks_per_sm = self.blocks_per_sm
         st.ring_slack = self.ring_slack
+        st.wait_spins = self.wait_spins
         L = lib()
         for key, with_pairs, lag in (("k", 1, self.lag), ("f", 0, self.lag_f)):
             nt = ctypes.c_int64()
@@ -208,6 +210,16 @@ class MeshPattern:
         on = self.split and d.get("n_gtasks_k", 0) > 0
         st.n_gtasks_k = d["n_gtasks_k"] if on else 0
         st.gtasks_k = d["gtasks_k"].data_ptr() if on else None
+
+    def set_wait_limit(self, spins: int) -> None:
+        """Polls after which a bounded wait of the persistent kernels gives up (0 = the
+        default of 1 << 22, about a second).  A wait that gives up sets status flag bit 0,
+        and the assembler then raises; the kernel itself always runs to its end."""
+        if int(spins) < 0:
+            raise ValueError("spins must be >= 0")
+        self.wait_spins = int(spins)
+        if self._dev is not None:
+            self._dev["plan"].wait_spins = self.wait_spins
 
     def set_queue(self, lag: int | None = None, blocks_per_sm: int | None = None,
                   ring_slack: int | None = None, lag_f: int | None = None, split: bool | None = None) -> None:

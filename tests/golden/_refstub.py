@@ -16,7 +16,8 @@ import os
 import sys
 import types
 
-REFERENCE_SRC = os.environ.get("PSIERRA_REFERENCE_SRC", "/root/reference/src")
+# the directory holding the reference package ``psierra`` (its ``src`` folder); required
+REFERENCE_SRC = os.environ.get("PSIERRA_REFERENCE_SRC", "")
 
 
 class _Anything:
@@ -66,6 +67,8 @@ class _StubFinder:
 def install() -> None:
     if "psierra" in sys.modules and getattr(sys.modules["psierra"], "_graft_stub", False):
         return
+    if not REFERENCE_SRC:
+        raise RuntimeError("set PSIERRA_REFERENCE_SRC to the reference's src directory (the one holding psierra/)")
     pkg_dir = os.path.join(REFERENCE_SRC, "psierra")
     if not os.path.isdir(pkg_dir):
         raise RuntimeError(f"reference sources not found at {pkg_dir}")

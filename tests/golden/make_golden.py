@@ -1,10 +1,10 @@
 """Generate the golden fixtures in ``tests/golden/`` by running the pSierra reference.
 
-Run in a container that has the reference sources (``PSIERRA_REFERENCE_SRC``,
-default ``/root/reference/src``)::
+Run in a container that has the reference sources, with ``PSIERRA_REFERENCE_SRC`` set
+to the reference's ``src`` directory (the one holding ``psierra/``)::
 
-    python tests/golden/make_golden.py            # all fixtures
-    python tests/golden/make_golden.py fbar_box   # one fixture that has its own seed
+    PSIERRA_REFERENCE_SRC=<reference>/src python tests/golden/make_golden.py            # all fixtures
+    PSIERRA_REFERENCE_SRC=<reference>/src python tests/golden/make_golden.py fbar_box   # one fixture
 
 Every output below comes from the reference's own classes (``Tet4TotalLagrangian``,
 ``Tet10TotalLagrangian``, ``NeoHookean``, ``SolidDomain``, ``NonlinearStaticAnalysis``,

@@ -99,6 +99,32 @@ def test_static_scratch_matches_workspace_entry_point(precond, aligned):
     assert np.linalg.norm(A @ x - b) < 1e-9 * np.linalg.norm(b)
 
 
+def test_static_call_after_the_first_reserves_no_device_memory():
+    # the first call has loaded the module and looked up the scratch address; a later
+    # call must leave the device's free memory unchanged (its outputs are allocated first)
+    L = _bind()
+    A, b = _system(False)
+    n = A.shape[0]
+    indptr, indices, vals, bd = _device(A, b)
+    st = torch.zeros(8, dtype=torch.int32, device="cuda")
+    x = torch.zeros_like(bd)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        rc = L.psx_pcg_static(n, indptr.data_ptr(), indices.data_ptr(), vals.data_ptr(), _lib.PSX_FP64,
+                              bd.data_ptr(), x.data_ptr(), 1e-10, 0.0, 20000, _lib.PSX_PRECOND_JACOBI,
+                              st.data_ptr(), stream)
+        assert rc == _lib.PSX_OK
+        torch.cuda.synchronize()
+
+    call()
+    free_before, _ = torch.cuda.mem_get_info()
+    call()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert int(st[5].item()) == 0
+
+
 def test_static_scratch_rejects_systems_beyond_its_size():
     L = _bind()
     cap = int(L.psx_pcg_static_max_bytes())
