@@ -236,6 +236,54 @@ def time_steps_flushed(fn, steps: int, warmup: int, sync_all, flush):
     return sum(a.elapsed_time(b) for a, b in ev) / steps
 
 
+# FP64 floating-point work of the FP64 f+K element sweep, per element: 2 x DFMA + DADD + DMUL
+# thread instructions of tet4_persistent_kernel<double, F|K> from the ncu counters
+# smsp__sass_thread_inst_executed_op_d{fma,add,mul}_pred_on.sum of one launch, divided by
+# its elements (None until measured).
+FP64_FLOPS_PER_ELEMENT = None
+
+
+def fp64_compute_roofline(E, ms, roofs):
+    """The FP64 sweep against its compute roof (FP64 FLOPs / time vs the FMA roof)."""
+    if FP64_FLOPS_PER_ELEMENT is None:
+        return {}
+    tf = FP64_FLOPS_PER_ELEMENT * E / (ms * 1e-3) / 1e12
+    return {"fp64_flops_per_element": FP64_FLOPS_PER_ELEMENT, "fp64_tflops": tf,
+            "fp64_compute_frac": tf / roofs["fp64_tflops"]}
+
+
+def compute_roofs(dev, iters: int = 40000, reps: int = 5):
+    """FP64 and FP32 CUDA-core FMA throughput of this GPU (TFLOP/s), measured with the
+    library's FMA kernel (psx_fma_roof): 8 resident blocks of 256 threads per SM, 8
+    independent FMA chains per thread, CUDA events around the launches."""
+    import ctypes
+
+    import torch
+
+    from psierra_b200 import _lib
+
+    L = _lib.lib()
+    blocks = 8 * torch.cuda.get_device_properties(dev).multi_processor_count
+    sink = torch.empty(int(L.psx_fma_roof_sink_bytes(blocks)), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    out = {}
+    for name, prec in (("fp64", _lib.PSX_FP64), ("fp32", _lib.PSX_FP32_MIXED)):
+        flops = ctypes.c_double()
+        for _ in range(2):
+            _lib.check(L.psx_fma_roof(prec, iters, blocks, _lib.ptr(sink), ctypes.byref(flops), stream), "psx_fma_roof")
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            _lib.check(L.psx_fma_roof(prec, iters, blocks, _lib.ptr(sink), ctypes.byref(flops), stream), "psx_fma_roof")
+        b.record()
+        torch.cuda.synchronize()
+        out[f"{name}_tflops"] = flops.value * reps / (a.elapsed_time(b) * 1e-3) / 1e12
+    out["method"] = (f"psx_fma_roof: {blocks} blocks x 256 threads, 8 independent FMA chains x {iters} steps per "
+                     f"thread, {reps} launches timed with CUDA events")
+    return out
+
+
 def peak_hbm():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -410,6 +458,7 @@ def main():
     bytes_fp64 = 16 * E + 48 * N + 8 * nnz + 24 * N
     bytes_kv = 16 * E + 96 * N
     peak, peak_kind = peak_hbm()
+    roofs = compute_roofs(dev)
     if pcg is not None:
         pcg["frac"] = pcg["gbs"] / peak
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
@@ -520,7 +569,9 @@ def main():
                          "launches_per_step": asm.launches_per_call("fp32-mixed")},
             "fp64": {"value": world * E / (ms_fp64 * 1e-3), "unit": "elements/s", "ms_per_step": ms_fp64,
                      "achieved_gbs": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9,
-                     "frac": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9 / peak},
+                     "frac": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9 / peak,
+                     **fp64_compute_roofline(E, ms_fp64, roofs)},
+            "compute_roofs": roofs,
             "mixed_over_fp64": ms_fp64 / ms_mixed,
             "kv": {"unit": "GB/s", "algorithmic_bytes_per_launch": bytes_kv,
                    "traffic": NCU_TRAFFIC["kv32"] * E / NCU_CAPTURE_ELEMENTS,

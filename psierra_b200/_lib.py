@@ -79,6 +79,10 @@ SIGNATURES: dict[str, list] = {
     "psx_tile_plan_fill": [_p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _p, _p],
     "psx_tile_meta_stride": [_i32],
     "psx_tet4_split_ready": [],
+    "psx_fma_roof": [_i32, _i64, _i32, _p, _p, _p],
+    "psx_fma_roof_sink_bytes": [_i32],
+    "psx_gather_pack_count": [_p, _i64, _p, _p, _p, _p],
+    "psx_gather_pack_fill": [_p, _i64, _p, _p, _p, _p, _p, _p, _p, _p],
 }
 
 
@@ -126,6 +130,8 @@ class PlanStruct(ctypes.Structure):
         ("gtasks_k", ctypes.c_void_p),
         ("wait_spins", ctypes.c_int32),
         ("reserved0", ctypes.c_int32),
+        ("gblk_k", ctypes.c_void_p),
+        ("gpack_k", ctypes.c_void_p),
     ]
 
 
@@ -150,6 +156,7 @@ def lib() -> ctypes.CDLL:
         L.psx_tile_meta_stride.restype = ctypes.c_int64
         L.psx_fbar_work_doubles.restype = ctypes.c_int64
         L.psx_ecsw_work_doubles.restype = ctypes.c_int64
+        L.psx_fma_roof_sink_bytes.restype = ctypes.c_int64
         _lib = L
     return _lib
 

@@ -88,46 +88,35 @@ __device__ __forceinline__ void neohookean_point(const double l[3][3], double mu
 #pragma unroll
     for (int j = 0; j < 3; ++j) s.F[i][j] = (i == j ? 1.0 : 0.0) + l[i][j];
   inv3(s.F, s.Finv);
-  // Green-Lagrange strain E = (l + l^T + l^T l) / 2 and its deviator.
+  // Green-Lagrange strain E = (l + l^T + l^T l) / 2 (symmetric: six entries formed)
   double E[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
+    for (int j = i; j < 3; ++j) {
       double ltl = l[0][i] * l[0][j] + l[1][i] * l[1][j] + l[2][i] * l[2][j];
       E[i][j] = 0.5 * (l[i][j] + l[j][i] + ltl);
+      E[j][i] = E[i][j];
     }
   double trE = E[0][0] + E[1][1] + E[2][2];
   s.I1 = 3.0 + 2.0 * trE;
-  // T = 2 phi dev E + beta I
+  // T = 2 phi dev E + beta I (symmetric)
   double T[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-      T[i][j] = 2.0 * s.phi * (E[i][j] - (i == j ? trE / 3.0 : 0.0)) + (i == j ? s.beta : 0.0);
-  // C^-1 = F^-1 F^-T
-  double Ci[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-      Ci[i][j] = s.Finv[i][0] * s.Finv[j][0] + s.Finv[i][1] * s.Finv[j][1] + s.Finv[i][2] * s.Finv[j][2];
-  // S = C^-1 T (symmetric: C^-1 and dev E commute), P = F S
-  double S[3][3];
+  const double tw = 2.0 * s.phi, dia = s.beta - tw * (trE / 3.0);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = i; j < 3; ++j) {
-      double v = Ci[i][0] * T[0][j] + Ci[i][1] * T[1][j] + Ci[i][2] * T[2][j];
-      S[i][j] = v;
-      S[j][i] = v;
+      T[i][j] = tw * E[i][j] + (i == j ? dia : 0.0);
+      T[j][i] = T[i][j];
     }
+  // S = C^-1 T, so P = F S = F F^-1 F^-T T = F^-T T: the first Piola stress without
+  // forming C^-1 or S
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j)
-      s.P[i][j] = s.F[i][0] * S[0][j] + s.F[i][1] * S[1][j] + s.F[i][2] * S[2][j];
+      s.P[i][j] = s.Finv[0][i] * T[0][j] + s.Finv[1][i] * T[1][j] + s.Finv[2][i] * T[2][j];
 }
 
 // Tangent coefficients with the integration weight folded in.

@@ -27,7 +27,7 @@ def declared_symbols() -> list[str]:
     names = []
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
-        names += re.findall(r"^\s*(?:int|size_t|void)\s+(psx_\w+)\s*\(", src, flags=re.M)
+        names += re.findall(r"^\s*(?:int|int64_t|size_t|void)\s+(psx_\w+)\s*\(", src, flags=re.M)
     return sorted(set(names))
 
 
