@@ -169,3 +169,58 @@ def test_ellipsoid_gravity_identification_gradient():
         with torch.no_grad():
             fd = (float(loss_of(mp)[0]) - float(loss_of(mm)[0])) / (2 * h)
         assert abs(g[e] - fd) <= 1e-5 * abs(fd) + 1e-12 * abs(float(L.detach())), (e, g[e], fd)
+
+
+def test_adjoint_parameter_derivatives_match_the_reference_element():
+    """w . df/dmu_e and w . df/dkappa_e of the adjoint kernel against the reference
+    element's force at (mu, kappa) = (1, 0) and (0, 1): the NeoHookean stress is linear in
+    the moduli at fixed F (material/neohookean.py:87-114), so these are the exact
+    derivatives of the reference's f_int."""
+    from oracle import equilibrium
+
+    m, asm, mu, kappa, rng = problem(seed=9, cells=(4, 3, 2))
+    u = 0.03 * rng.normal(size=(m.n_nodes, 3))
+    w = rng.normal(size=m.n_dofs)
+    _, gmu, gka = asm.adjoint(torch.from_numpy(u.reshape(-1)).to(DEV), torch.from_numpy(w).to(DEV))
+    rmu, rka = equilibrium.force_parameter_gradients(m.nodes, m.elements, u, w)
+    assert np.abs(gmu.cpu().numpy() - rmu).max() <= 1e-11 * np.abs(rmu).max()
+    assert np.abs(gka.cpu().numpy() - rka).max() <= 1e-11 * np.abs(rka).max()
+
+
+def test_equilibrium_gradient_matches_reference_forward_model():
+    """dL/dmu_e through StaticEquilibrium (device Newton + adjoint PCG) against central
+    differences h = 1e-6 mu_e of the reference forward model: the oracle's Newton with the
+    direct solver on the reference element and assembly (oracle/equilibrium.py, pinned to
+    the reference's own Newton run), the way the reference identifies parameters
+    (inverse/parameter_identification.py:346-383).  kappa = 50 mu moves with mu; the target
+    displacement comes from a second seeded mu field; 32 random elements; 1e-5 relative."""
+    from oracle import equilibrium
+
+    m, asm, mu, kappa, rng = problem(seed=13, cells=(4, 2, 2))
+    clamp = meshgen.nodes_on_plane(m, 0, "min")
+    fixed = np.concatenate([3 * clamp + c for c in range(3)])
+    f_np = meshgen.traction_nodal_forces(m, 0, "max", [0.0, 0.0, -8.0])
+    f_ext = torch.from_numpy(f_np).to(DEV)
+    mu_tgt = np.exp(np.log(1000.0) + 0.3 * np.random.default_rng(14).normal(size=m.n_elements))
+    u_tgt = equilibrium.solve_static(m.nodes, m.elements, mu_tgt, 50.0 * mu_tgt, fixed, f_np)
+    obs = np.setdiff1d(np.arange(m.n_dofs), fixed)
+
+    def ref_loss(mu_np):
+        u = equilibrium.solve_static(m.nodes, m.elements, mu_np, 50.0 * mu_np, fixed, f_np)
+        return 0.5 * float(np.sum((u[obs] - u_tgt[obs]) ** 2))
+
+    nt = DeviceNewton(asm, fixed, precision="fp64", pcg_tol=1e-13)
+    mt = torch.from_numpy(mu).to(DEV).requires_grad_(True)
+    u = static_equilibrium(nt, mt, 50.0 * mt, f_ext, n_steps=2, nr_tol=1e-12, polish=3)
+    obs_t = torch.from_numpy(obs).to(DEV)
+    L = 0.5 * torch.sum((u[obs_t] - torch.from_numpy(u_tgt[obs]).to(DEV)) ** 2)
+    L.backward()
+    g = mt.grad.cpu().numpy()
+    assert abs(float(L.detach()) - ref_loss(mu)) <= 1e-8 * ref_loss(mu)
+    for e in rng.choice(m.n_elements, size=32, replace=False):
+        h = 1e-6 * mu[e]
+        mp, mm = mu.copy(), mu.copy()
+        mp[e] += h
+        mm[e] -= h
+        fd = (ref_loss(mp) - ref_loss(mm)) / (2 * h)
+        assert abs(g[e] - fd) <= 1e-5 * abs(fd) + 1e-12 * float(L.detach()) / mu[e], (e, g[e], fd)
