@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-fbar", action="store_true", help="skip the Tet4Fbar assembly measurement")
     ap.add_argument("--no-pcg", action="store_true", help="skip the PCG iteration measurement")
     ap.add_argument("--no-oracle", action="store_true", help="skip the accuracy check against the oracle")
+    ap.add_argument("--dr-iterations", type=int, default=1000,
+                    help="fused dynamic-relaxation pseudo-steps timed per precision (0 = skip)")
     ap.add_argument("--oracle-nodes", type=int, default=2000, help="nodes whose rows the oracle checks")
     return ap.parse_args()
 
@@ -236,6 +238,61 @@ def time_steps_flushed(fn, steps: int, warmup: int, sync_all, flush):
     return sum(a.elapsed_time(b) for a, b in ev) / steps
 
 
+def dr_benchmark(asm, k_vals, u_dev, m, iterations: int, sync_all):
+    """The workload's dynamic relaxation: ``iterations`` fused matrix-free pseudo-steps
+    (K_T(u) x on the fly, the viscous update of psierra analysis/dynamic_relaxation.py:
+    296-299, 378-382 with damping c = 0.1, dt = 1), per precision, on the cube clamped at
+    z = 0 with the reference's Gerschgorin lumped mass (dynamic_relaxation.py:87-128,
+    safety factor 1.1) built from the assembled tangent.  One launch per pseudo-step; the
+    working set (connectivity, X, u and five DOF vectors, ~150 MB) exceeds the L2."""
+    import torch
+
+    dev = u_dev.device
+    n = 3 * m.n_nodes
+    indptr = torch.from_numpy(asm.pattern.indptr.astype(np.int64)).to(dev)
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), indptr[1:] - indptr[:-1])
+    row = torch.zeros(n, dtype=torch.float64, device=dev).index_add_(0, rows, k_vals.abs().double())
+    del rows
+    dt, sf, c = 1.0, 1.1, 0.1
+    mdiag = 0.25 * sf * dt * dt * torch.clamp(row, min=1e-6 * float(row.max()))
+    minv = 1.0 / mdiag
+    zfix = np.flatnonzero(np.isclose(m.nodes[:, 2], 0.0))
+    minv[torch.from_numpy(np.concatenate([3 * zfix + k for k in range(3)])).to(dev)] = 0.0
+    c1, c2 = (2 - c * dt) / (2 + c * dt), 2 * dt / (2 + c * dt)
+    b = torch.from_numpy(np.random.default_rng(5).standard_normal(n)).to(dev)
+    b.mul_(minv != 0)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    vel = torch.zeros_like(x)
+    E, N = m.n_elements, m.n_nodes
+    # conn, X, u; x read, b, 1/m, vel read + write, x write
+    bytes_it = 16 * E + 48 * N + 24 * N * 6
+    out = {"workload": "cube 80^3 clamped at z = 0, Gerschgorin lumped mass (sf 1.1), damping 0.1, dt 1; "
+                       f"{iterations} fused K(u)-matrix-free pseudo-steps (psx_tet4_dr_step) per precision",
+           "iterations": iterations, "algorithmic_bytes_per_iteration": bytes_it}
+    for prec in ("fp32-mixed", "fp64"):
+        x.zero_()
+        vel.zero_()
+        for _ in range(5):
+            asm.dr_step(u_dev, b, minv, x, vel, c1, c2, dt, precision=prec, check_status=False)
+        x.zero_()
+        vel.zero_()
+        sync_all()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(iterations):
+            asm.dr_step(u_dev, b, minv, x, vel, c1, c2, dt, precision=prec, check_status=False)
+        e.record()
+        torch.cuda.synchronize()
+        asm.raise_on_bad_elements(u_dev)
+        ms = a.elapsed_time(e)
+        r = b - asm.kv(u_dev, x, precision="fp64")
+        out[prec.replace("-", "_")] = {
+            "ms_total": ms, "ms_per_iteration": ms / iterations, "gbs": bytes_it * iterations / (ms * 1e-3) / 1e9,
+            "relative_residual_after": float((r * (minv != 0)).norm() / b.norm())}
+    return out
+
+
 # FP64 floating-point work of the FP64 f+K element sweep, per element: 2 x DFMA + DADD + DMUL
 # thread instructions of tet4_persistent_kernel<double, F|K> from the ncu counters
 # smsp__sass_thread_inst_executed_op_d{fma,add,mul}_pred_on.sum of one launch, divided by
@@ -390,6 +447,10 @@ def main():
                                  args.steps, args.warmup, sync_all, flush)
     del scrub
 
+    dr = None
+    if args.dr_iterations > 0:
+        dr = dr_benchmark(asm, k32, u_dev, m, args.dr_iterations, sync_all)
+
     if world > 1:
         t = torch.tensor([ms_mixed, ms_fp64], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -444,12 +505,19 @@ def main():
 
         ms_it = ms_per_iteration(_lib.PSX_PCG_NODAL)
         ms_row = ms_per_iteration(0)
-        # CSR values (fp32) + indices once, ~7 vectors of n doubles (p, q, x, r, z, and the
-        # preconditioner's 3x3 blocks ~ 3 n doubles)
-        bytes_it = 8 * nnz + 8 * 7 * n + 8 * 3 * n
+        # Bytes the node-blocked format must move per iteration: the FP32 values once, one
+        # column index per 3x3 block (nnz / 9: the three rows of a node share their column
+        # list), and ~10 vectors of n doubles (p, q, x, r, z and the 3x3 preconditioner
+        # blocks, 3 n).  The row-wise CSR equivalent (a column index per value) is beside it.
+        bytes_it = 4 * nnz + 4 * (nnz // 9) + 8 * 10 * n
+        bytes_csr = 8 * nnz + 8 * 10 * n
         pcg = {"workload": "block-Jacobi PCG on the FP32-mixed tangent of the same mesh, clamped at z = 0, "
                            "fixed iteration count, node-blocked SpMV (PSX_PCG_NODAL)", "ms_per_iteration": ms_it,
                "algorithmic_bytes_per_iteration": bytes_it, "gbs": bytes_it / (ms_it * 1e-3) / 1e9,
+               "bytes_note": "frac is on the node-blocked bytes (values + nnz/9 indices + vectors); "
+                             "csr_equivalent_frac charges a column index per value",
+               "csr_equivalent_bytes_per_iteration": bytes_csr,
+               "csr_equivalent_gbs": bytes_csr / (ms_it * 1e-3) / 1e9,
                "kernels_per_iteration": 3, "row_spmv_ms_per_iteration": ms_row}
         del kc, pw
 
@@ -461,6 +529,11 @@ def main():
     roofs = compute_roofs(dev)
     if pcg is not None:
         pcg["frac"] = pcg["gbs"] / peak
+        pcg["csr_equivalent_frac"] = pcg["csr_equivalent_gbs"] / peak
+    if dr is not None:
+        for v in dr.values():
+            if isinstance(v, dict) and "gbs" in v:
+                v["frac"] = v["gbs"] / peak
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
 
     # Tet10: cube 30^3 Kuhn split upgraded to 10 nodes (162,000 elements, 226,981 nodes,
@@ -586,6 +659,7 @@ def main():
             "tet10": tet10,
             "fbar": fbar,
             "pcg": pcg,
+            "dynamic_relaxation": dr,
             "cpu_baseline": cb, "e2e": e2e, "gpu_launches": args.steps * asm.launches_per_call("fp32-mixed"),
             "gpu_launches_note": "assembly timed region; each K.v step is one launch as well",
             "clocks": clk,
