@@ -293,8 +293,10 @@ int psx_tet4_assemble(const psx_plan_t* plan, const double* X, const double* u,
  * Tet10 Total-Lagrangian NeoHookean assembly, 4-point rule (replaces the element loops of
  * domain/solid.py:172-207, 230-325 around element/tet10_total_lagrangian.py:63-136 and
  * element/tet10_base.py:310-342).  Same arguments and outputs as psx_tet4_assemble;
- * modes PSX_WANT_F, PSX_WANT_K, PSX_LINEAR.  The plan must be built with npe = 10 and an
- * element task tile of 8.
+ * modes PSX_WANT_F, PSX_WANT_K, PSX_LINEAR and PSX_MASS (the consistent mass of
+ * element/tet10_base.py:344-372 with the corner tetrahedron's |det| / 6 as the element
+ * volume, density in `lam`).  The plan must be built with npe = 10 and an element task
+ * tile of 8.
  */
 int psx_tet10_assemble(const psx_plan_t* plan, const double* X, const double* u,
                        const double* mu_e, const double* kappa_e, double mu, double kappa, double lam,

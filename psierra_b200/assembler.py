@@ -75,6 +75,7 @@ class GPUAssembler:
         self.rho = float(getattr(material, "mass_density", 0.0) or 0.0)
         self.mu_e = self._per_element(getattr(material, "mu_e", None))
         self.kappa_e = self._per_element(getattr(material, "kappa_e", None))
+        self._const_mats = {}  # M and K_0 of the composed effective tangent depend on the material
 
     def _per_element(self, a):
         if a is None:
@@ -145,8 +146,6 @@ class GPUAssembler:
         prec = precision or self.precision
         if prec not in PRECISIONS:
             raise ValueError(f"unknown precision {prec!r}")
-        if self.npe == 10 and mass:
-            raise NotImplementedError("the Tet10 consistent mass is assembled on the host by the reference domain")
         if linear or mass:
             mode = _lib.PSX_MASS if mass else _lib.PSX_LINEAR
             want_f, want_k, linear = False, True, True
@@ -185,10 +184,13 @@ class GPUAssembler:
         constants, ``c_t = 1 - alpha_f``, ``c_m = (1 - alpha_m) a0 + (1 - alpha_f) a1 alpha_R``
         and ``c_0 = (1 - alpha_f) a1 beta_R`` for Rayleigh damping ``alpha_R M + beta_R K_0``.
         ``M`` is the consistent mass of density ``rho`` (default: the material's) and ``K_0``
-        the small-strain stiffness of the material.
+        the small-strain stiffness of the material.  Tet4 forms all three in one fused
+        sweep; Tet10 assembles K_T in one sweep and adds M and K_0, assembled once on the
+        same pattern and cached, with one in-place axpy over the CSR values.
         """
         if self.npe != 4:
-            raise NotImplementedError("the fused effective tangent is a Tet4 sweep")
+            return self._effective_composed(u, c_t, c_m, c_0, rho, want_f, precision or self.precision, f_out, k_out,
+                                            check_status)
         prec = precision or self.precision
         u = self._check_u(u)
         if want_f and f_out is None:
@@ -208,6 +210,32 @@ class GPUAssembler:
         if check_status:
             self.raise_on_bad_elements(u)
         return (f_out if want_f else None), k_out
+
+    def _effective_composed(self, u, c_t, c_m, c_0, rho, want_f, prec, f_out, k_out, check_status):
+        """c_t K_T(u) + c_m M + c_0 K_0 from one K_T sweep and the cached M, K_0 (Tet10)."""
+        if c_0 != 0.0 and self.mu_e is not None:
+            raise NotImplementedError("the Tet10 small-strain stiffness takes scalar moduli")
+        rho = self.rho if rho is None else float(rho)
+        f_out, k_out = self.assemble(u, want_f=want_f, want_k=True, precision=prec, f_out=f_out, k_out=k_out,
+                                     check_status=check_status)
+        cache = self.__dict__.setdefault("_const_mats", {})
+        if c_m != 0.0:
+            key = ("M", prec, rho)
+            if key not in cache:
+                saved, self.rho = self.rho, rho
+                try:
+                    cache[key] = self.assemble(None, mass=True, precision=prec)[1]
+                finally:
+                    self.rho = saved
+            k_out.mul_(c_t).add_(cache[key], alpha=c_m)
+        else:
+            k_out.mul_(c_t)
+        if c_0 != 0.0:
+            key = ("K0", prec)
+            if key not in cache:
+                cache[key] = self.assemble(None, linear=True, precision=prec)[1]
+            k_out.add_(cache[key], alpha=c_0)
+        return f_out, k_out
 
     def kv(self, u: torch.Tensor, v: torch.Tensor, precision: str | None = None,
            y_out: torch.Tensor | None = None, check_status: bool = True) -> torch.Tensor:

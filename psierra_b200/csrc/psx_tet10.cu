@@ -41,6 +41,16 @@ __constant__ PairTable c_pairs = {
     {1, 2, 3, 4, 5, 6, 7, 8, 9, 2, 3, 4, 5, 6, 7, 8, 9, 3, 4, 5, 6, 7, 8, 9, 4, 5, 6, 7, 8, 9, 5, 6, 7, 8, 9, 6, 7, 8, 9,
      7, 8, 9, 8, 9, 9, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9}};
 
+// Consistent mass of the 10-node tetrahedron with straight edges: M_ab = rho V m_ab / 2520
+// times the 3x3 identity, m_ab the exact integrals of N_a N_b over the reference element
+// (VTK node order; element/tet10_base.py:11-27, 344-372).
+__constant__ int16_t c_mass10[10][10] = {
+    {36, 6, 6, 6, -24, -36, -24, -24, -36, -36},   {6, 36, 6, 6, -24, -24, -36, -36, -24, -36},
+    {6, 6, 36, 6, -36, -24, -24, -36, -36, -24},   {6, 6, 6, 36, -36, -36, -36, -24, -24, -24},
+    {-24, -24, -36, -36, 192, 96, 96, 96, 96, 48}, {-36, -24, -24, -36, 96, 192, 96, 48, 96, 96},
+    {-24, -36, -24, -36, 96, 96, 192, 96, 48, 96}, {-24, -36, -36, -24, 96, 48, 96, 192, 96, 96},
+    {-36, -24, -36, -24, 96, 96, 48, 96, 192, 96}, {-36, -36, -24, -24, 48, 96, 96, 96, 96, 192}};
+
 // Barycentric coordinates (L1, L2, L3) of the 4-point rule: a = (5 - sqrt 5)/20,
 // b = (5 + 3 sqrt 5)/20.
 __device__ __forceinline__ void qp_coords(int q, double& L1, double& L2, double& L3) {
@@ -94,6 +104,39 @@ __device__ __forceinline__ void tet10_tile(const Tet10Args& A, const int4& task,
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0 && !kLinear;
   constexpr bool kWantK = (MODE & PSX_WANT_K) != 0 || kLinear;
   const int lane = threadIdx.x & 31;
+  if constexpr ((MODE & PSX_MASS) != 0) {
+    // consistent mass (density in lam0) with the element volume of the mesh, |det| / 6 of
+    // the corner tetrahedron (domain/solid.py:209-228): one 3x3 block per lane
+    const int n = (int)(task.w - task.z);
+    for (int t = lane; t < n * 55; t += 32) {
+      const int me = t / 55, slot = t - me * 55;
+      const int a = c_pairs.a[slot], b = c_pairs.b[slot];
+      const int64_t em = task.z + me;
+      double Xc[4][3];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double* x = A.X + 3 * (int64_t)__ldg(A.conn + 10 * em + c);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) Xc[c][i] = __ldg(x + i);
+      }
+      double D[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) D[i][j] = Xc[j + 1][i] - Xc[0][i];
+      const double V = fabs(det3(D)) / 6.0;
+      const KT m = (KT)(A.lam0 * V * (double)c_mass10[a][b] / 2520.0);
+      KT* rec = krec + (em & ring_mask) * L10::kK;
+      if (slot < 45) {
+        const KT blk[9] = {m, (KT)0, (KT)0, (KT)0, m, (KT)0, (KT)0, (KT)0, m};
+        store_pair_block<KT>(rec + L10::pair_off(slot), blk, false);
+      } else {
+        const KT dg[6] = {m, (KT)0, (KT)0, m, (KT)0, m};
+        store_diag_block<KT>(rec + L10::diag_off(slot - 45), dg);
+      }
+    }
+    return;
+  }
   const int le = lane >> 2, q = lane & 3;
   const int64_t e = task.z + (int64_t)le;
   const bool active = e < task.w;
@@ -266,7 +309,7 @@ __global__ void __launch_bounds__(kThreads10, 2)
 tet10_persistent_kernel(Tet10Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ krec, double* __restrict__ frec,
                         KT* __restrict__ k_out, double* __restrict__ f_out) {
   constexpr bool kWantF = (MODE & PSX_WANT_F) != 0;
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0;
   extern __shared__ __align__(16) unsigned char s_raw[];
   Tet10Smem<KT>& sm = reinterpret_cast<Tet10Smem<KT>*>(s_raw)[threadIdx.x >> 5];
   auto element_tile = [&](const int4& task) { tet10_tile<KT, MODE>(A, task, g.ring_mask, krec, frec, sm); };
@@ -307,7 +350,7 @@ __global__ void tet10_dets_kernel(const int32_t* __restrict__ conn, const double
 template <typename KT, int MODE>
 int run_tet10(const psx_plan_t* P, const Tet10Args& A, const WorkLayout& W, KT* k_out, double* f_out,
               cudaStream_t stream) {
-  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR)) != 0;
+  constexpr bool kWantK = (MODE & (PSX_WANT_K | PSX_LINEAR | PSX_MASS)) != 0;
   const GatherArgs g = gather_args(P, W.ring_elems);
   const QueueArgs Q = queue_args(P, W, kWantK);
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
@@ -331,8 +374,9 @@ extern "C" int psx_tet10_assemble(const psx_plan_t* plan, const double* X, const
   using namespace psx;
   if (!plan || plan->npe != 10 || !X || !status || !work || plan->tile != kTile10) return PSX_ERR_ARG;
   const bool wantF = (mode & PSX_WANT_F) != 0, wantK = (mode & PSX_WANT_K) != 0,
-             linear = (mode & PSX_LINEAR) != 0;
-  if (mode & ~(PSX_WANT_F | PSX_WANT_K | PSX_LINEAR)) return PSX_ERR_ARG;
+             mass = (mode & PSX_MASS) != 0, linear = (mode & PSX_LINEAR) != 0 || mass;
+  if (mode & ~(PSX_WANT_F | PSX_WANT_K | PSX_LINEAR | PSX_MASS)) return PSX_ERR_ARG;
+  if ((mode & PSX_LINEAR) && mass) return PSX_ERR_ARG;
   if (linear && (wantF || wantK || !k_out)) return PSX_ERR_ARG;
   if (!linear && (!(wantF || wantK) || !u)) return PSX_ERR_ARG;
   if (wantF && !f_out) return PSX_ERR_ARG;
@@ -344,6 +388,7 @@ extern "C" int psx_tet10_assemble(const psx_plan_t* plan, const double* X, const
   Tet10Args A{plan->conn, X, u, mu_e, kappa_e, mu, kappa, lam, static_cast<Status*>(status)};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 #define PSX_T10(KT, M) run_tet10<KT, M>(plan, A, W, static_cast<KT*>(k_out), f_out, s)
+  if (mass) return precision == PSX_FP64 ? PSX_T10(double, PSX_MASS) : PSX_T10(float, PSX_MASS);
   if (linear) return precision == PSX_FP64 ? PSX_T10(double, PSX_LINEAR) : PSX_T10(float, PSX_LINEAR);
   if (wantF && wantK)
     return precision == PSX_FP64 ? PSX_T10(double, PSX_WANT_F | PSX_WANT_K)

@@ -51,8 +51,6 @@ class DeviceGeneralizedAlpha:
     def __init__(self, asm: GPUAssembler, fixed_dofs, damping=(0.0, 0.0), spectral_radius: float = 0.8,
                  precision: str | None = None, pcg_tol: float = 1e-12, pcg_maxiter: int = 20000,
                  preconditioner: str = "block-jacobi"):
-        if asm.npe != 4:
-            raise NotImplementedError("the device dynamics driver runs the Tet4 effective tangent")
         if not (0.0 <= spectral_radius <= 1.0):
             raise ValueError(f"spectral_radius must be in [0.0, 1.0], got {spectral_radius}")
         rho = float(spectral_radius)

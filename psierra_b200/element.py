@@ -111,6 +111,7 @@ class _GPUElementBase:
         self._material = mat
         if self._asm is not None:
             self._asm.set_material(mat)
+        self.__dict__.pop("_one", None)  # the cached one-element assembler holds the old material
         self._last_u = None
 
     @property
@@ -228,28 +229,52 @@ class _GPUElementBase:
         """(k_tan, f_int) of one element (psierra ``element/tet4_total_lagrangian.py:77-139``).
 
         Runs the same GPU kernel on a one-element mesh; it exists for API
-        compatibility, while the domain hooks above are the throughput path.
+        compatibility (reference code that loops over elements, such as the ECSW model or
+        a per-element mass loop, calls it once per element), while the domain hooks above
+        are the throughput path.  The one-element mesh, its pattern, plan and workspace are
+        built on the first call and reused: a later call only uploads the element's
+        coordinates, displacements and, with per-element moduli, its mu and kappa.
         """
-        from psierra_b200.meshgen import TetMesh
-
-        X = np.asarray(node_coords, dtype=np.float64).reshape(self._npe, 3)
-        mat = self._material
-        if elem_index is not None and getattr(mat, "mu_e", None) is not None:
-            from psierra_b200.material import NeoHookeanField, _host
-
-            mat = NeoHookeanField(np.asarray(_host(mat.mu_e))[[elem_index]],
-                                  np.asarray(_host(mat.kappa_e))[[elem_index]])
-        one = type(self)(mat, precision=self.precision, device=self.device)
-        mesh = TetMesh(X, np.arange(self._npe, dtype=np.int64)[None, :])
-        f, K = one.assemble_force_and_tangent(mesh, np.asarray(u_nodes, dtype=np.float64))
+        one, mesh = self._single_element(node_coords, elem_index)
+        f, K = one.assemble_force_and_tangent(mesh, np.asarray(u_nodes, dtype=np.float64).reshape(self._npe, 3))
         return K.toarray(), f
 
-    def compute_linear_stiffness_matrix(self, node_coords, elem_index=None, **kw):
+    def _single_element(self, node_coords, elem_index):
+        """(element, mesh) of the cached one-element assembler, set to this element."""
+        from psierra_b200.material import _host
         from psierra_b200.meshgen import TetMesh
 
         X = np.asarray(node_coords, dtype=np.float64).reshape(self._npe, 3)
-        one = type(self)(self._material, precision=self.precision, device=self.device)
-        return one.assemble_stiffness_matrix(TetMesh(X, np.arange(self._npe, dtype=np.int64)[None, :])).toarray()
+        from psierra_b200.material import NeoHookeanField
+
+        mat = self._material
+        one_mat = mat
+        if getattr(mat, "mu_e", None) is not None:
+            if elem_index is None:
+                raise ValueError("per-element moduli need elem_index")
+            pick = lambda a: np.asarray(_host(a), dtype=np.float64)[[elem_index]]  # noqa: E731
+            lam = getattr(mat, "lam_e", None)
+            one_mat = NeoHookeanField(pick(mat.mu_e), pick(mat.kappa_e), mass_density=mat.mass_density,
+                                      lam_e=None if lam is None else pick(lam))
+        cached = self.__dict__.get("_one")
+        if cached is None:
+            mesh = TetMesh(X.copy(), np.arange(self._npe, dtype=np.int64)[None, :])
+            one = type(self)(one_mat, precision=self.precision, device=self.device)
+            one._setup(mesh)
+            cached = self._one = (one, mesh)
+        one, mesh = cached
+        asm = one._setup(mesh)
+        mesh.nodes[:] = X
+        asm.X.copy_(torch.from_numpy(X))
+        if one_mat is not mat:
+            asm.set_material(one_mat)
+        return one, mesh
+
+    def compute_linear_stiffness_matrix(self, node_coords, elem_index=None, **kw):
+        """Small-strain k_e of one element (psierra ``element/tet4_base.py:129-136``), on the
+        cached one-element assembler."""
+        one, mesh = self._single_element(node_coords, elem_index)
+        return one.assemble_stiffness_matrix(mesh).toarray()
 
 
 class Tet4TotalLagrangian(_GPUElementBase):
@@ -294,8 +319,6 @@ class Tet10TotalLagrangian(_GPUElementBase):
         rho = self._material.mass_density
         return np.kron(_TET10_MASS_INT / 2520.0 * rho * volume, np.identity(3))
 
-    def assemble_mass_matrix(self, mesh):
-        raise NotImplementedError("the Tet10 consistent mass is assembled by SolidDomain.assemble_mass_matrix")
 
 
 class Tet4Fbar(_GPUElementBase):

@@ -187,6 +187,23 @@ def dynamic_fixture():
                 lam=mat.parameters.lame_parameter_1)
 
 
+def dynamic_tet10_fixture():
+    """NonlinearDynamicAnalysis with Tet10TotalLagrangian on a small cantilever (6 x 2 x 2
+    cells -> 144 Tet10): the same load and integrator settings as dynamic_fixture, plus
+    the consistent mass the reference domain assembles (element/tet10_base.py:344-372)."""
+    mb = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 0.1, 0.1, 6, 2, 2))
+    mat = nh(1e5, 0.3, rho=1000.0)
+    dm, f_ext, clamp = cantilever_problem(mb, -50.0)
+    dom = SolidDomain(DuckMesh(mb.nodes, mb.elements), mat, Tet10TotalLagrangian(mat))
+    M = dom.assemble_mass_matrix()
+    an = NonlinearDynamicAnalysis(dom, damping=RayleighDamping(0.5, 1e-4), spectral_radius=0.8)
+    r = an.solve(dirichlet=dm, f_ext=f_ext, dt=0.05, n_steps=8, nr_iterations=15, nr_tol=1e-8, verbose=False)
+    return dict(u=dom.u.copy(), v=dom.v.copy(), a=dom.a.copy(), iterations=np.array(r.iteration_history),
+                converged=r.converged, f_ext=f_ext, clamp=clamp, dt=0.05, n_steps=8, rho=1000.0,
+                rayleigh=np.array([0.5, 1e-4]), spectral_radius=0.8, nr_tol=1e-8,
+                M_data=M.data, M_indptr=M.indptr, M_indices=M.indices)
+
+
 def tet10_newton_fixture():
     """The Tet10 cube solve at a reduced grid (3^3 cells -> 162 Tet10): clamp z = 0,
     u_z = -0.2 prescribed on z = 1 and ramped over 8 increments (nonlinear_static.py:
@@ -210,7 +227,8 @@ def main(only=None):
     out = {}
     if only:
         # fixtures that need no shared random stream can be regenerated on their own
-        gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture, "tet10_newton": tet10_newton_fixture}
+        gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture, "tet10_newton": tet10_newton_fixture,
+                "dynamic_tet10": dynamic_tet10_fixture}
         for name in only:
             out[name] = gens[name]()
         for name, d in out.items():
@@ -322,6 +340,7 @@ def main(only=None):
     out["fbar_box"] = fbar_fixture()
     out["dynamic_beam"] = dynamic_fixture()
     out["tet10_newton"] = tet10_newton_fixture()
+    out["dynamic_tet10"] = dynamic_tet10_fixture()
 
     for name, d in out.items():
         path = os.path.join(HERE, f"{name}.npz")

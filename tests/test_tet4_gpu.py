@@ -186,3 +186,22 @@ def test_negative_volume_raises_reference_error():
     el = Tet4TotalLagrangian(nh(10e3, 0.45))
     with pytest.raises(ValueError, match="Negative or zero element volume detected"):
         el.assemble_internal_forces(bad, np.zeros((m.n_nodes, 3)))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32-mixed"])
+def test_per_element_api_reuses_one_assembler(precision):
+    """compute_nonlinear_force_and_tangent_stiffness / compute_linear_stiffness_matrix called
+    element by element on one object (as reference loops over elements do): the cached
+    one-element assembler is built once and gives each golden element's k, f and k_lin."""
+    g = golden("element_tet4")
+    el = Tet4TotalLagrangian(NeoHookeanField(g["mu"], g["kappa"], lam_e=g["lam"]), precision=precision)
+    ktol = 1e-12 if precision == "fp64" else 1e-6
+    first = None
+    for i in range(16):
+        k, f = el.compute_nonlinear_force_and_tangent_stiffness(g["X"][i], g["u"][i], elem_index=i)
+        assert rel_max(k, g["k"][i]) < ktol and rel_max(f, g["f"][i]) < 5e-12
+        kl = el.compute_linear_stiffness_matrix(g["X"][i], elem_index=i)
+        assert rel_max(kl, g["k_lin"][i]) < ktol
+        one = el._one[0]._asm
+        first = first or one
+        assert one is first  # built once
