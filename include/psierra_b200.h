@@ -165,11 +165,6 @@ typedef struct psx_plan {
      lets a test make a wait run out without faulting the GPU. */
   int32_t wait_spins;
   int32_t reserved0;        /* 0 */
-  /* Packed gather blocks of gtasks_k (psx_gather_pack_fill; device; required with
-     gtasks_k): per gather task 4 int32 (kind | count << 8, granule, first 16-byte chunk,
-     chunk count) and the chunks themselves. */
-  const int32_t* gblk_k;
-  const uint8_t* gpack_k;
 } psx_plan_t;
 
 /* n_pairs = (sum deg - N) / 2 and the pair_src length E * npe (npe - 1) / 2 (host). */
@@ -213,23 +208,6 @@ int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32_t tile, co
                        const int32_t* pair_src, int64_t n_pairs, const int32_t* node_ptr, const int32_t* node_src,
                        int64_t N, uint8_t* meta, int32_t* pair_ptr_t, int32_t* pair_src_t, int32_t* node_ptr_t,
                        int32_t* node_src_t, int32_t* caps);
-
-/*
- * Packed gather blocks of the warp-specialised Tet4 kernel (host; no counterpart in the
- * reference): for each of the n_gtasks gather tasks (4 int32 each: kind 1 = pairs or 2 =
- * nodes, granule, first item, end item; at most 32 items) one contiguous run of 16-byte
- * chunks holding the items' info rows (chunks 0-31), 33 uint16 offsets of their codes
- * (chunks 32-36) and the codes (pair_src_t / node_src_t) from chunk 37 on, so that a
- * gather warp fetches the whole task with one asynchronous copy.  count: total chunks
- * and the largest block (PSX_ERR_LIMIT if a task holds more than 65,535 codes or the
- * total reaches 2^31 chunks).  fill: blk (4 n_gtasks: kind | count << 8, granule, first
- * chunk, chunk count) and pack (16 total_chunks bytes).
- */
-int psx_gather_pack_count(const int32_t* gtasks, int64_t n_gtasks, const int32_t* pair_ptr_t,
-                          const int32_t* node_ptr_t, int64_t* total_chunks, int32_t* max_chunks);
-int psx_gather_pack_fill(const int32_t* gtasks, int64_t n_gtasks, const int32_t* pair_info,
-                         const int32_t* pair_ptr_t, const int32_t* pair_src_t, const int32_t* node_info,
-                         const int32_t* node_ptr_t, const int32_t* node_src_t, int32_t* blk, uint8_t* pack);
 
 /*
  * F-bar plan (host; Tet4Fbar, element/tet4_fbar.py:53-118, 420-459): the two-ring graph

@@ -81,8 +81,6 @@ SIGNATURES: dict[str, list] = {
     "psx_tet4_split_ready": [],
     "psx_fma_roof": [_i32, _i64, _i32, _p, _p, _p],
     "psx_fma_roof_sink_bytes": [_i32],
-    "psx_gather_pack_count": [_p, _i64, _p, _p, _p, _p],
-    "psx_gather_pack_fill": [_p, _i64, _p, _p, _p, _p, _p, _p, _p, _p],
 }
 
 
@@ -130,8 +128,6 @@ class PlanStruct(ctypes.Structure):
         ("gtasks_k", ctypes.c_void_p),
         ("wait_spins", ctypes.c_int32),
         ("reserved0", ctypes.c_int32),
-        ("gblk_k", ctypes.c_void_p),
-        ("gpack_k", ctypes.c_void_p),
     ]
 
 

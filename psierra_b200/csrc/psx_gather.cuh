@@ -57,27 +57,7 @@ struct GatherArgs {
   const uint8_t* tile_meta;
   int32_t meta_stride, off_p, off_n, src_p, src_n;
   int32_t tile;
-  // packed gather blocks of the warp-specialised kernel (psx_gather_pack_fill)
-  const int4* gblk;
-  const uint4* gpack;
 };
-
-// Asynchronous global -> shared copies (no registers held while in flight).  The 16-byte
-// form bypasses L1; the 8-byte form (the only one below 16 bytes) allocates in L1.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // 16-byte vector loads/stores of record blocks (L2-only loads: the ring is rewritten while
 // the kernel runs, so nothing may be served from a stale L1 line).
@@ -574,193 +554,6 @@ __device__ __forceinline__ void drain_gathers(const GatherArgs& g, const QueueAr
   }
 }
 
-// ---- packed gather blocks (warp-specialised kernel) -----------------------------------
-// A gather task's block (psx_gather_pack_fill): chunks 0-31 the items' info rows, chunks
-// 32-36 the 33 uint16 offsets of their codes, codes from chunk 37 on.  Blocks of up to
-// kGatherStageChunks chunks are copied into shared memory one task ahead; a larger block
-// is read where it lies in global memory.
-constexpr int kPackHeadChunks = 37;
-constexpr int kGatherStageChunks = 104;  // 1,664 bytes: up to 268 codes per task
-
-struct GatherStage {
-  uint4 buf[2][kGatherStageChunks];
-};
-
-__device__ __forceinline__ void stage_gather_block(GatherStage& gs, int b, const GatherArgs& g, const int4& blk) {
-  const int lane = threadIdx.x & 31;
-  if (blk.w > kGatherStageChunks) return;
-  const uint4* src = g.gpack + blk.z;
-  for (int c = lane; c < blk.w; c += 32) cp_async16(&gs.buf[b][c], src + c);
-}
-
-// Pair item from its tile-record codes (ascending tile order): the off-diagonal block K_ij
-// written to the row segments of 3i+k and, transposed, of 3j+m (tile records hold FP32 K).
-template <int BATCH>
-__device__ __forceinline__ void gather_pair_codes(const GatherArgs& g, const int4& info, const int32_t* codes, int n,
-                                                  const float* __restrict__ krec, float* __restrict__ k_out) {
-  float acc[9];
-#pragma unroll
-  for (int j = 0; j < 9; ++j) acc[j] = 0.f;
-  for (int s = 0; s < n; s += BATCH) {
-    int32_t src[BATCH];
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b) src[b] = (s + b < n) ? codes[s + b] : -1;
-    float v[BATCH][9];
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b)
-      if (src[b] >= 0) {
-        const float* base = krec + ((int64_t)(src[b] >> 8) & g.ring_tile_mask) * g.tile_k;
-        const int lp = src[b] & 255;
-        const float4 x = __ldcg(reinterpret_cast<const float4*>(base) + lp);
-        const float4 y = __ldcg(reinterpret_cast<const float4*>(base + 4 * g.cap_p4) + lp);
-        v[b][0] = x.x; v[b][1] = x.y; v[b][2] = x.z; v[b][3] = x.w;
-        v[b][4] = y.x; v[b][5] = y.y; v[b][6] = y.z; v[b][7] = y.w;
-        v[b][8] = __ldcg(base + 8 * g.cap_p4 + lp);
-      }
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b)
-      if (src[b] >= 0) {
-#pragma unroll
-        for (int j = 0; j < 9; ++j) acc[j] += v[b][j];
-      }
-  }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) store3(k_out + info.x + (int64_t)info.y * k, acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]);
-#pragma unroll
-  for (int m = 0; m < 3; ++m) store3(k_out + info.z + (int64_t)info.w * m, acc[m], acc[3 + m], acc[6 + m]);
-}
-
-// Node item from its tile-record codes: the diagonal block and / or f of the node.
-template <bool WANT_K, bool WANT_F, int BATCH>
-__device__ __forceinline__ void gather_node_codes(const GatherArgs& g, const int4& info, const int32_t* codes, int n,
-                                                  const float* __restrict__ krec, const double* __restrict__ frec,
-                                                  float* __restrict__ k_out, double* __restrict__ f_out) {
-  float acc[6];
-#pragma unroll
-  for (int j = 0; j < 6; ++j) acc[j] = 0.f;
-  double fa[3] = {0.0, 0.0, 0.0};
-  for (int s = 0; s < n; s += BATCH) {
-    int32_t src[BATCH];
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b) src[b] = (s + b < n) ? codes[s + b] : -1;
-    float v[BATCH][6];
-    double fv[BATCH][3];
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b)
-      if (src[b] >= 0) {
-        const int64_t slot = (int64_t)(src[b] >> 7) & g.ring_tile_mask;
-        const int ln = src[b] & 127;
-        if constexpr (WANT_K) {
-          const float* base = krec + slot * g.tile_k + 9 * g.cap_p4;
-          const float4 x = __ldcg(reinterpret_cast<const float4*>(base) + ln);
-          const float2 y = __ldcg(reinterpret_cast<const float2*>(base + 4 * g.cap_n4) + ln);
-          v[b][0] = x.x; v[b][1] = x.y; v[b][2] = x.z; v[b][3] = x.w;
-          v[b][4] = y.x; v[b][5] = y.y;
-        }
-        if constexpr (WANT_F) {
-          const double* fb = frec + slot * 3 * g.cap_n4 + ln;
-          fv[b][0] = __ldcg(fb);
-          fv[b][1] = __ldcg(fb + g.cap_n4);
-          fv[b][2] = __ldcg(fb + 2 * g.cap_n4);
-        }
-      }
-#pragma unroll
-    for (int b = 0; b < BATCH; ++b)
-      if (src[b] >= 0) {
-        if constexpr (WANT_K) {
-#pragma unroll
-          for (int j = 0; j < 6; ++j) acc[j] += v[b][j];
-        }
-        if constexpr (WANT_F) {
-          fa[0] += fv[b][0];
-          fa[1] += fv[b][1];
-          fa[2] += fv[b][2];
-        }
-      }
-  }
-  if constexpr (WANT_K) {
-    if (info.y > 0) {
-      const float full[9] = {acc[0], acc[1], acc[2], acc[1], acc[3], acc[4], acc[2], acc[4], acc[5]};
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-        store3(k_out + info.x + (int64_t)info.y * k, full[3 * k], full[3 * k + 1], full[3 * k + 2]);
-    }
-  }
-  if constexpr (WANT_F) {
-    __stcs(f_out + 3 * (int64_t)info.z + 0, fa[0]);
-    __stcs(f_out + 3 * (int64_t)info.z + 1, fa[1]);
-    __stcs(f_out + 3 * (int64_t)info.z + 2, fa[2]);
-  }
-}
-
-// Gather role of the warp-specialised kernel on packed blocks.  Tasks are claimed in list
-// order two ahead: while task t is summed, the block of task t+1 is copied into the other
-// stage buffer and the block descriptor of task t+2 is loaded, so that a task's only
-// dependent global loads are its tile records.  The waits are those of drain_gathers, and
-// the earliest unfinished task is always some warp's current task, so the queues drain.
-template <bool WANT_K, bool WANT_F, int PAIR_BATCH, int NODE_BATCH>
-__device__ __forceinline__ void drain_gathers_packed(const GatherArgs& g, const QueueArgs& Q, int32_t n_gtasks,
-                                                     int32_t* gcnt, Status* st, GatherStage& gs,
-                                                     const float* __restrict__ krec, const double* __restrict__ frec,
-                                                     float* __restrict__ k_out, double* __restrict__ f_out) {
-  const int lane = threadIdx.x & 31;
-  int32_t* acnt = Q.counters + 1;
-  int32_t* bcnt = Q.counters + 1 + Q.n_granules;
-  const int64_t gsize = (int64_t)1 << Q.granule_log2;
-  auto atiles = [&](int32_t r) -> int32_t {
-    const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
-    return (int32_t)((n + Q.tile - 1) / Q.tile);
-  };
-  auto claim = [&]() -> int32_t {
-    int32_t v = 0;
-    if (lane == 0) v = atomicAdd(gcnt, 1);
-    return __shfl_sync(0xffffffffu, v, 0);
-  };
-  const int4 none = make_int4(0, 0, 0, 0);
-  int32_t t = claim();
-  int32_t tn = claim();
-  int4 blk = t < n_gtasks ? __ldg(g.gblk + t) : none;
-  int4 blkn = tn < n_gtasks ? __ldg(g.gblk + tn) : none;
-  if (t < n_gtasks) stage_gather_block(gs, 0, g, blk);
-  cp_async_commit();
-  int32_t next = 0;
-  if (lane == 0) next = atomicAdd(gcnt, 1);
-  int b = 0;
-  while (t < n_gtasks) {
-    const int32_t tnn = __shfl_sync(0xffffffffu, next, 0);
-    if (lane == 0) next = atomicAdd(gcnt, 1);
-    const int4 blknn = tnn < n_gtasks ? __ldg(g.gblk + tnn) : none;
-    const int32_t gr = blk.y;
-    const int32_t first = max(0, gr - Q.span_g - 1);
-    wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
-    cp_async_wait_group<0>();  // this task's block
-    __syncwarp();
-    if (tn < n_gtasks) stage_gather_block(gs, b ^ 1, g, blkn);
-    cp_async_commit();
-    const uint4* base = blk.w <= kGatherStageChunks ? gs.buf[b] : g.gpack + blk.z;
-    const int kind = blk.x & 255, count = blk.x >> 8;
-    if (lane < count) {
-      const int4 info = reinterpret_cast<const int4*>(base)[lane];
-      const uint16_t* off = reinterpret_cast<const uint16_t*>(base + 32);
-      const int32_t* codes = reinterpret_cast<const int32_t*>(base + kPackHeadChunks);
-      const int c0 = off[lane], c1 = off[lane + 1];
-      if (kind == 1) {
-        if constexpr (WANT_K) gather_pair_codes<PAIR_BATCH>(g, info, codes + c0, c1 - c0, krec, k_out);
-      } else {
-        gather_node_codes<WANT_K, WANT_F, NODE_BATCH>(g, info, codes + c0, c1 - c0, krec, frec, k_out, f_out);
-      }
-    }
-    __syncwarp();
-    if (lane == 0) atomicAdd(bcnt + gr, 1);
-    t = tn;
-    tn = tnn;
-    blk = blkn;
-    blkn = blknn;
-    b ^= 1;
-  }
-  cp_async_wait_group<0>();
-}
-
 inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
   GatherArgs g;
   g.pair_info = P->pair_info;
@@ -792,8 +585,6 @@ inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
     g.meta_stride = (g.src_n + 4 * T + 15) / 16 * 16;
   }
   g.ring_tile_mask = P->tile > 0 ? ring_elems / P->tile - 1 : 0;
-  g.gblk = reinterpret_cast<const int4*>(P->gblk_k);
-  g.gpack = reinterpret_cast<const uint4*>(P->gpack_k);
   return g;
 }
 

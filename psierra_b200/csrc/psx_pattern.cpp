@@ -444,79 +444,6 @@ extern "C" int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32
 }
 
 // ---------------------------------------------------------------------------
-// Packed gather blocks of the warp-specialised Tet4 kernel: per gather task (items
-// [first, last) of one kind and granule, at most 32), one contiguous run of 16-byte
-// chunks that a gather warp copies into shared memory ahead of time:
-//   chunks [0, 32)  the items' info rows (pair_info / node_info), slot i = item first + i;
-//   chunks [32, 37) 33 uint16 offsets of each item's codes within the code area;
-//   chunks [37, ..) the codes themselves (pair_src_t / node_src_t), int32, zero-padded.
-// blk[4 t .. 4 t + 3] = (kind | count << 8, granule, first chunk, chunk count).
-namespace {
-constexpr int64_t kPackHead = 37;
-int64_t pack_codes(const int32_t* task, const int32_t* pair_ptr_t, const int32_t* node_ptr_t) {
-  const int32_t* ptr = task[0] == 1 ? pair_ptr_t : node_ptr_t;
-  return (int64_t)ptr[task[3]] - ptr[task[2]];
-}
-bool pack_task_ok(const int32_t* task) {
-  return (task[0] == 1 || task[0] == 2) && task[2] >= 0 && task[3] > task[2] && task[3] - task[2] <= 32;
-}
-}  // namespace
-
-extern "C" int psx_gather_pack_count(const int32_t* gtasks, int64_t n_gtasks, const int32_t* pair_ptr_t,
-                                     const int32_t* node_ptr_t, int64_t* total_chunks, int32_t* max_chunks) {
-  if (!gtasks || n_gtasks < 0 || !pair_ptr_t || !node_ptr_t || !total_chunks || !max_chunks) return PSX_ERR_ARG;
-  int64_t tot = 0, mx = 0;
-  for (int64_t t = 0; t < n_gtasks; ++t) {
-    const int32_t* task = gtasks + 4 * t;
-    if (!pack_task_ok(task)) return PSX_ERR_ARG;
-    const int64_t codes = pack_codes(task, pair_ptr_t, node_ptr_t);
-    if (codes < 0 || codes > 65535) return PSX_ERR_LIMIT;  // uint16 offsets
-    const int64_t n = kPackHead + (codes + 3) / 4;
-    tot += n;
-    mx = std::max(mx, n);
-  }
-  if (tot >= ((int64_t)1 << 31)) return PSX_ERR_LIMIT;
-  *total_chunks = tot;
-  *max_chunks = (int32_t)mx;
-  return PSX_OK;
-}
-
-extern "C" int psx_gather_pack_fill(const int32_t* gtasks, int64_t n_gtasks, const int32_t* pair_info,
-                                    const int32_t* pair_ptr_t, const int32_t* pair_src_t, const int32_t* node_info,
-                                    const int32_t* node_ptr_t, const int32_t* node_src_t, int32_t* blk,
-                                    uint8_t* pack) {
-  if (!gtasks || n_gtasks < 0 || !pair_info || !pair_ptr_t || !pair_src_t || !node_info || !node_ptr_t ||
-      !node_src_t || !blk || !pack)
-    return PSX_ERR_ARG;
-  int64_t chunk = 0;
-  for (int64_t t = 0; t < n_gtasks; ++t) {
-    const int32_t* task = gtasks + 4 * t;
-    if (!pack_task_ok(task)) return PSX_ERR_ARG;
-    const bool pairs = task[0] == 1;
-    const int32_t* info = pairs ? pair_info : node_info;
-    const int32_t* ptr = pairs ? pair_ptr_t : node_ptr_t;
-    const int32_t* src = pairs ? pair_src_t : node_src_t;
-    const int32_t first = task[2], count = task[3] - task[2];
-    const int64_t codes = pack_codes(task, pair_ptr_t, node_ptr_t);
-    const int64_t n = kPackHead + (codes + 3) / 4;
-    uint8_t* b = pack + 16 * chunk;
-    std::memset(b, 0, (size_t)(16 * n));
-    std::memcpy(b, info + 4 * (int64_t)first, (size_t)16 * count);
-    uint16_t* off = reinterpret_cast<uint16_t*>(b + 16 * 32);
-    int32_t* code = reinterpret_cast<int32_t*>(b + 16 * kPackHead);
-    const int32_t base = ptr[first];
-    for (int32_t i = 0; i <= count; ++i) off[i] = (uint16_t)(ptr[first + i] - base);
-    std::memcpy(code, src + base, (size_t)4 * codes);
-    blk[4 * t + 0] = task[0] | (count << 8);
-    blk[4 * t + 1] = task[1];
-    blk[4 * t + 2] = (int32_t)chunk;
-    blk[4 * t + 3] = (int32_t)n;
-    chunk += n;
-  }
-  return PSX_OK;
-}
-
-// ---------------------------------------------------------------------------
 // F-bar plan (Tet4Fbar, element/tet4_fbar.py:53-118, 420-459).  The nodal volumetric
 // blocks kappa v0_a g_a g_a^T couple every two nodes of node a's element patch, so the
 // tangent lives on the two-ring graph: b ~ c when some node a neighbours both.  For

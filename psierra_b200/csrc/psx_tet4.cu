@@ -119,17 +119,9 @@ __device__ __forceinline__ void put_diag(KT* __restrict__ krec, int o, const KT 
   }
 }
 
-// Element inputs staged in shared memory by the warp-specialised kernel (PRELOADED): the
-// connectivity and the nodal X, u of the element, copied there ahead of time.
-struct Tet4Inputs {
-  int4 cn;
-  double X[4][3];
-  double U[4][3];
-};
-
-template <typename KT, int MODE, bool KGLOBAL = true, bool FGLOBAL = true, bool PRELOADED = false>
+template <typename KT, int MODE, bool KGLOBAL = true, bool FGLOBAL = true>
 __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
-                                             double* __restrict__ frec, const Tet4Inputs* in = nullptr) {
+                                             double* __restrict__ frec) {
   using L = RecLayout<4>;
   constexpr bool kAdj = (MODE & kModeAdjoint) != 0;
   constexpr bool kKV = (MODE & PSX_KV) != 0 || kAdj;
@@ -137,27 +129,15 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
   constexpr bool kMass = (MODE & PSX_MASS) != 0;
   constexpr bool kWantK = ((MODE & PSX_WANT_K) != 0 || kLinear) && !kKV;
-  int4 cn;
+  const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
   double Xn[4][3];
-  double Un[4][3];
+  load_nodes(A.X, cn, Xn);
   // sweeps forming a tangent or K.v load the displacements with the coordinates (one
   // round trip to memory); the f-only sweep, with fewer registers in use, is faster
   // loading them after the geometry
-  constexpr bool kEarlyU = PRELOADED || (!kMass && !kLinear && (kWantK || kKV));
-  if constexpr (PRELOADED) {
-    cn = in->cn;
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        Xn[b][k] = in->X[b][k];
-        Un[b][k] = in->U[b][k];
-      }
-  } else {
-    cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
-    load_nodes(A.X, cn, Xn);
-    if constexpr (kEarlyU) load_nodes(A.U, cn, Un);
-  }
+  constexpr bool kEarlyU = !kMass && !kLinear && (kWantK || kKV);
+  double Un[4][3];
+  if constexpr (kEarlyU) load_nodes(A.U, cn, Un);
   Tet4Geom G;
   tet4_geometry(Xn, G);
   if (!(G.detD > 0.0)) flag_bad_element(A.st, e, true);
@@ -514,39 +494,12 @@ struct Tet4Smem {
   static constexpr size_t kWarpBytes = sizeof(float) * kKFloats + sizeof(double) * kFDoubles + kMeta;
 };
 
-// Inputs of the element tiles of one warp of the warp-specialised kernel, copied ahead:
-// the connectivity of the next two tiles (double-buffered) and the nodal X and u of the
-// next tile, component-major so that lane-consecutive loads hit consecutive banks.
-struct ElemInputStage {
-  int4 conn[2][32];
-  double xu[24][32];  // [6 b + k][lane]: X of element node b (k < 3), u (k >= 3)
-};
-
-// Copy tile t's connectivity into conn[buf] (one 16-byte copy per lane).
-__device__ __forceinline__ void stage_conn(ElemInputStage& st, int buf, const int32_t* conn, int64_t t, int64_t E) {
-  const int lane = threadIdx.x & 31;
-  const int64_t e = t * 32 + lane;
-  if (e < E) cp_async16(&st.conn[buf][lane], reinterpret_cast<const int4*>(conn) + e);
+// Asynchronous 16-byte global -> shared copies (no registers held while in flight).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
-
-// Copy the nodal X and u of tile t, whose connectivity is already staged in conn[buf].
-__device__ __forceinline__ void stage_nodes(ElemInputStage& st, int buf, const double* X, const double* U, int64_t t,
-                                            int64_t E) {
-  const int lane = threadIdx.x & 31;
-  if (t * 32 + lane >= E) return;
-  const int4 c = st.conn[buf][lane];
-  const int ids[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    const double* x = X + 3 * (int64_t)ids[b];
-    const double* u = U + 3 * (int64_t)ids[b];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      cp_async8(&st.xu[6 * b + k][lane], x + k);
-      cp_async8(&st.xu[6 * b + 3 + k][lane], u + k);
-    }
-  }
-}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Start copying tile t's meta block into the warp's list area.
 __device__ __forceinline__ void tile_meta_prefetch(const GatherArgs& g, int64_t t, unsigned char* lst) {
@@ -740,88 +693,27 @@ tet4_split_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, const int4* __restrict_
   int32_t* gcnt = Q.counters + 1 + 2 * Q.n_granules;
   if (warp < kSplitElemWarps) {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kSplitElemRegs));
-    unsigned char* my_stage = s_stage + warp * (S::kWarpBytes + sizeof(ElemInputStage));
+    unsigned char* my_stage = s_stage + warp * S::kWarpBytes;
     float* kst = reinterpret_cast<float*>(my_stage);
     double* fst = reinterpret_cast<double*>(my_stage + sizeof(float) * S::kKFloats);
     unsigned char* lst = my_stage + sizeof(float) * S::kKFloats + sizeof(double) * S::kFDoubles;
-    ElemInputStage& in_st = *reinterpret_cast<ElemInputStage*>(my_stage + S::kWarpBytes);
-    // Element tiles (32 elements, one per lane) are claimed in index order two ahead.
-    // While tile tA is evaluated, the nodal inputs of tile tB and the connectivity of
-    // tile tC are copied into shared memory (cp.async), so that no evaluation waits on a
-    // global load.  Copy groups: [lists of tA] then [inputs of tB, conn of tC]; the first
-    // is awaited before tA's reduction, the second at the top of the next iteration.
-    // The ring wait guards only the tile-record writes of the reduction, so it sits just
-    // before them.  Claims are in index order, so the earliest unfinished tile is always
-    // some warp's current tile and the queues still drain (the waits of drain_elements).
-    int32_t* acnt = Q.counters + 1;
-    int32_t* bcnt = Q.counters + 1 + Q.n_granules;
-    auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
-    const int64_t E = Q.n_elements;
-    const int64_t n_tiles = (E + 31) / 32;
-    auto claim = [&]() -> int32_t {
-      int32_t v = 0;
-      if (lane == 0) v = atomicAdd(ecnt, 1);
-      return __shfl_sync(0xffffffffu, v, 0);
-    };
-    int32_t tA = claim();
-    int32_t tB = claim();
-    if (tA < n_tiles) stage_conn(in_st, 0, A.conn, tA, E);
-    cp_async_commit();
-    cp_async_wait_group<0>();
-    __syncwarp();
-    if (tA < n_tiles) stage_nodes(in_st, 0, A.X, A.U, tA, E);
-    if (tB < n_tiles) stage_conn(in_st, 1, A.conn, tB, E);
-    cp_async_commit();
-    int32_t next = 0;
-    if (lane == 0) next = atomicAdd(ecnt, 1);
-    int cur = 0;
-    while (tA < n_tiles) {
-      cp_async_wait_group<0>();
+    drain_elements(Q, ecnt, A.st, [&](const int4& task) {
+      const int64_t t = task.z / g.tile;
+      tile_meta_prefetch(g, t, lst);
+      const int64_t e = task.z + (int64_t)lane;
+      if (e < task.w)
+        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
+                                             fst + kFStride * lane);
+      cp_async_wait_all();
       __syncwarp();
-      const int64_t e = (int64_t)tA * 32 + lane;
-      Tet4Inputs in;
-      if (e < E) {
-        in.cn = in_st.conn[cur][lane];
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            in.X[b][k] = in_st.xu[6 * b + k][lane];
-            in.U[b][k] = in_st.xu[6 * b + 3 + k][lane];
-          }
-      }
-      __syncwarp();  // every lane holds its inputs: the node stage and conn[cur] are free
-      const int32_t tC = __shfl_sync(0xffffffffu, next, 0);
-      if (lane == 0) next = atomicAdd(ecnt, 1);
-      tile_meta_prefetch(g, tA, lst);
-      cp_async_commit();
-      if (tB < n_tiles) stage_nodes(in_st, cur ^ 1, A.X, A.U, tB, E);
-      if (tC < n_tiles) stage_conn(in_st, cur, A.conn, tC, E);
-      cp_async_commit();
-      if (e < E)
-        tet4_element<KT, MODE, false, false, true>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
-                                                   fst + kFStride * lane, &in);
-      cp_async_wait_group<1>();  // the lists of tA; the next tile's inputs may still be in flight
-      const int32_t gr = (int32_t)(((int64_t)tA * 32) >> Q.granule_log2);
-      const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, A.st, Q.max_spins);
+      tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
       __syncwarp();
-      tile_reduce<S::kWantK, S::kWantF>(g, tA, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
-      __syncwarp();
-      if (lane == 0) publish_tile(acnt + gr);
-      tA = tB;
-      tB = tC;
-      cur ^= 1;
-    }
-    cp_async_wait_group<0>();
+    });
   } else {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kSplitGatherRegs));
     constexpr int kPairBatch = S::kWantF ? PSX_SPLIT_PAIR_BATCH_FK : PSX_SPLIT_PAIR_BATCH_K;
-    GatherStage& gs = reinterpret_cast<GatherStage*>(
-        s_stage + kSplitElemWarps * (S::kWarpBytes + sizeof(ElemInputStage)))[warp - kSplitElemWarps];
-    drain_gathers_packed<S::kWantK, S::kWantF, kPairBatch, PSX_SPLIT_NODE_BATCH>(
-        g, Q, n_gtasks, gcnt, A.st, gs, reinterpret_cast<const float*>(krec), frec, reinterpret_cast<float*>(k_out),
-        f_out);
+    drain_gathers<KT, 4, S::kWantK, S::kWantF, kPairBatch, PSX_SPLIT_NODE_BATCH>(
+        g, Q, gtasks, n_gtasks, gcnt, A.st, krec, frec, k_out, f_out);
   }
 }
 
@@ -899,13 +791,10 @@ int run_tet4_split(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, 
   using S = Tet4Smem<KT, MODE>;
   const GatherArgs g = gather_args(P, W.ring_elems);
   const QueueArgs Q = queue_args(P, W, true);
-  // one element per lane: the element tiles are exactly one warp wide
-  if (!W.tiles || !S::kTiles || P->tile != 32 || g.tile_k % 4 || g.meta_stride > kMetaBytes) return PSX_ERR_ARG;
-  if (!P->gtasks_k || !P->gblk_k || !P->gpack_k || P->n_gtasks_k <= 0 || P->n_gtasks_k > 0x7fffffff)
-    return PSX_ERR_ARG;
+  if (!W.tiles || !S::kTiles || P->tile > 32 || g.tile_k % 4 || g.meta_stride > kMetaBytes) return PSX_ERR_ARG;
+  if (!P->gtasks_k || P->n_gtasks_k <= 0 || P->n_gtasks_k > 0x7fffffff) return PSX_ERR_ARG;
   if (cudaMemsetAsync(W.counters, 0, W.counter_bytes, stream) != cudaSuccess) return PSX_ERR_CUDA;
-  const size_t smem = kSplitElemWarps * (S::kWarpBytes + sizeof(ElemInputStage)) +
-                      (kSplitThreads / 32 - kSplitElemWarps) * sizeof(GatherStage);
+  const size_t smem = kSplitElemWarps * S::kWarpBytes;
   static unsigned long long s_smem_set = 0;
   if (set_dynamic_smem_once(tet4_split_kernel<KT, MODE>, (int)smem, &s_smem_set) != cudaSuccess) return PSX_ERR_CUDA;
   const int grid = device_sm_count();  // one block (the whole register file) per SM
@@ -922,8 +811,7 @@ int run_tet4_split(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, 
 template <int MODE>
 int run_tet4_k32(const psx_plan_t* P, const Tet4Args& A, const WorkLayout& W, float* k_out, double* f_out,
                  cudaStream_t stream) {
-  if (P->gtasks_k && P->gblk_k && P->gpack_k && P->n_gtasks_k > 0 && W.tiles && P->tile == 32 &&
-      split_usable<float, MODE>())
+  if (P->gtasks_k && P->n_gtasks_k > 0 && W.tiles && split_usable<float, MODE>())
     return run_tet4_split<float, MODE>(P, A, W, k_out, f_out, stream);
   return run_tet4<float, MODE>(P, A, W, k_out, f_out, stream);
 }

@@ -203,34 +203,13 @@ class MeshPattern:
                 gk = np.ascontiguousarray(tk[tk[:, 0] != 0])
                 d["gtasks_k"] = t(gk.reshape(-1) if gk.size else np.zeros(4, dtype=np.int32))
                 d["n_gtasks_k"] = int(gk.shape[0])
-                if gk.size:
-                    blk, pack = self._gather_pack(gk)
-                    d["gblk_k"], d["gpack_k"] = t(blk), t(pack)
         self._apply_split(d)
-
-    def _gather_pack(self, gk: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-        """Packed per-task gather blocks of the warp-specialised kernel (``psx_gather_pack_fill``)."""
-        h = self.plan_host()
-        L = lib()
-        n = int(gk.shape[0])
-        total = ctypes.c_int64()
-        biggest = ctypes.c_int32()
-        check(L.psx_gather_pack_count(ptr(gk), n, ptr(h["pair_ptr_t"]), ptr(h["node_ptr_t"]), ctypes.byref(total),
-                                      ctypes.byref(biggest)), "psx_gather_pack_count")
-        blk = np.zeros(4 * n, dtype=np.int32)
-        pack = np.zeros(16 * int(total.value), dtype=np.uint8)
-        check(L.psx_gather_pack_fill(ptr(gk), n, ptr(h["pair_info"]), ptr(h["pair_ptr_t"]), ptr(h["pair_src_t"]),
-                                     ptr(h["node_info"]), ptr(h["node_ptr_t"]), ptr(h["node_src_t"]), ptr(blk),
-                                     ptr(pack)), "psx_gather_pack_fill")
-        return blk, pack
 
     def _apply_split(self, d: dict) -> None:
         st = d["plan"]
         on = self.split and d.get("n_gtasks_k", 0) > 0
         st.n_gtasks_k = d["n_gtasks_k"] if on else 0
         st.gtasks_k = d["gtasks_k"].data_ptr() if on else None
-        st.gblk_k = d["gblk_k"].data_ptr() if on else None
-        st.gpack_k = d["gpack_k"].data_ptr() if on else None
 
     def set_wait_limit(self, spins: int) -> None:
         """Polls after which a bounded wait of the persistent kernels gives up (0 = the

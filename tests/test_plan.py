@@ -193,55 +193,3 @@ def test_tile_plan_gather_reproduces_coo_sum(name):
         tiles = h["pair_src_t"][h["pair_ptr_t"][q]:h["pair_ptr_t"][q + 1]] >> 8
         assert np.all(np.diff(tiles) > 0)
     assert h["tile_caps"][0] <= 6 * T and h["tile_caps"][1] <= 4 * T
-
-
-def _task_lists(name, lag=2):
-    """Gather tasks of the K queue and the packed blocks the warp-specialised kernel reads."""
-    import ctypes
-
-    from psierra_b200 import _lib
-
-    m = MESHES[name]() if name in MESHES else meshgen.box_tet4(1.0, 1.0, 1.0, 12, 12, 12)
-    p = MeshPattern(m.elements, m.n_nodes)
-    p.lag = lag
-    h = p.plan_host()
-    st = _lib.PlanStruct()
-    st.npe, st.n_granules, st.n_elements, st.n_nodes = 4, h["n_granules"], m.n_elements, m.n_nodes
-    st.granule, st.max_span, st.n_pairs = p.granule, int(h["max_span"][0]), h["n_pairs"]
-    st.pair_gptr, st.node_gptr = h["pair_gptr"].ctypes.data, h["node_gptr"].ctypes.data
-    L = _lib.lib()
-    nt = ctypes.c_int64()
-    _lib.check(L.psx_task_count(ctypes.byref(st), 1, p.tile, p.tile_items, lag, ctypes.byref(nt)), "count")
-    tasks = np.zeros(4 * int(nt.value), dtype=np.int32)
-    btiles = np.zeros(h["n_granules"], dtype=np.int32)
-    _lib.check(L.psx_task_fill(ctypes.byref(st), 1, p.tile, p.tile_items, lag, _lib.ptr(tasks), _lib.ptr(btiles)),
-               "fill")
-    tk = tasks.reshape(-1, 4)
-    gk = np.ascontiguousarray(tk[tk[:, 0] != 0])
-    blk, pack = p._gather_pack(gk)
-    return h, gk, blk.reshape(-1, 4), pack
-
-
-@pytest.mark.parametrize("name", ["cfg1", "unstructured", "cube12"])
-def test_gather_pack_blocks_hold_each_task_items_and_codes(name):
-    h, gk, blk, pack = _task_lists(name)
-    chunk = 0
-    for t in range(gk.shape[0]):
-        kind, gr, z, w = (int(v) for v in gk[t])
-        count = w - z
-        assert blk[t, 0] == kind | (count << 8) and blk[t, 1] == gr and blk[t, 2] == chunk
-        b = pack[16 * chunk:16 * (chunk + blk[t, 3])]
-        info = b[:512].view(np.int32).reshape(32, 4)
-        off = b[512:512 + 66].view(np.uint16)
-        codes = b[16 * 37:].view(np.int32)
-        src_info = h["pair_info"] if kind == 1 else h["node_info"]
-        ptr_t = h["pair_ptr_t"] if kind == 1 else h["node_ptr_t"]
-        src_t = h["pair_src_t"] if kind == 1 else h["node_src_t"]
-        assert np.array_equal(info[:count], src_info.reshape(-1, 4)[z:w])
-        assert not info[count:].any()
-        for i in range(count):
-            want = src_t[ptr_t[z + i]:ptr_t[z + i + 1]]
-            assert np.array_equal(codes[off[i]:off[i + 1]], want)
-        assert blk[t, 3] == 37 + (int(off[count]) + 3) // 4
-        chunk += int(blk[t, 3])
-    assert 16 * chunk == pack.size

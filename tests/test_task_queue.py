@@ -89,16 +89,13 @@ def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
             assert (srcs // granule).min() >= g - span_g - 1 and (srcs // granule).max() <= g
 
 
-@pytest.mark.parametrize("depth", [1, 3])
 @pytest.mark.parametrize("granule,lag,workers,seed", [(128, 0, (1, 1), 0), (128, 2, (3, 2), 1), (256, 4, (2, 5), 2),
                                                       (64, 0, (4, 4), 3)])
-def test_split_queues_drain(granule, lag, workers, seed, depth):
+def test_split_queues_drain(granule, lag, workers, seed):
     """The warp-specialised kernel's two queues: element tiles claimed in index order by
     element warps, the gather tasks of the K queue claimed in order by gather warps, with
-    the same waits.  Each warp claims up to ``depth`` tasks ahead (the kernel claims two
-    ahead, to stage their inputs) and works them in claim order.  A random schedule of a
-    few workers per role must always drain, and a gather tile may only run once every
-    element tile of its span is done."""
+    the same waits.  A random schedule of a few workers per role must always drain, and
+    a gather tile may only run once every element tile of its span is done."""
     m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
     p = MeshPattern(m.elements, m.n_nodes)
     p.granule = granule
@@ -114,8 +111,8 @@ def test_split_queues_drain(granule, lag, workers, seed, depth):
     done_a = np.zeros(G, dtype=np.int64)
     done_b = np.zeros(G, dtype=np.int64)
     nxt = {"e": 0, "g": 0}
-    held = {("e", i): [] for i in range(workers[0])}
-    held.update({("g", i): [] for i in range(workers[1])})
+    held = {("e", i): None for i in range(workers[0])}
+    held.update({("g", i): None for i in range(workers[1])})
     rng = np.random.default_rng(seed)
 
     def ready(role, t):
@@ -128,20 +125,20 @@ def test_split_queues_drain(granule, lag, workers, seed, depth):
     remaining = n_tiles + len(gtasks)
     while remaining:
         moves = []
-        for w, q in held.items():
+        for w, t in held.items():
             role = w[0]
-            if len(q) < depth and nxt[role] < (n_tiles if role == "e" else len(gtasks)):
-                moves.append((w, "claim"))
-            if q and ready(role, q[0]):
-                moves.append((w, "run"))
+            if t is None:
+                if nxt[role] < (n_tiles if role == "e" else len(gtasks)):
+                    moves.append(w)
+            elif ready(role, t):
+                moves.append(w)
         assert moves, "split queues deadlocked"
-        w, what = moves[rng.integers(len(moves))]
-        role = w[0]
-        if what == "claim":
-            held[w].append(nxt[role])
+        w = moves[rng.integers(len(moves))]
+        role, t = w[0], held[w]
+        if t is None:
+            held[w] = nxt[role]
             nxt[role] += 1
         else:
-            t = held[w].pop(0)
             if role == "e":
                 done_a[t * tile // granule] += 1
             else:
@@ -149,6 +146,7 @@ def test_split_queues_drain(granule, lag, workers, seed, depth):
                 # everything this gather tile reads is complete
                 assert all(done_a[r] >= atiles[r] for r in range(max(0, g - span_g - 1), g + 1))
                 done_b[g] += 1
+            held[w] = None
             remaining -= 1
     assert (done_a == np.array(atiles)).all() and (done_b == bt).all()
 
