@@ -324,7 +324,8 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
 // ---------------------------------------------------------------------------
 // Tile plan (Tet4): the element tile of one warp (T consecutive elements) sums the
 // blocks its elements share before anything leaves the SM.  Per tile, the distinct
-// node pairs (and nodes) get local indices in order of first occurrence; for each
+// node pairs (and nodes) get local indices by descending contribution count, ties in
+// order of first occurrence; for each
 // local pair the tile lists its contributions (element-in-tile * 8 + slot) in element
 // order.  Everything one tile needs is one contiguous block (psx_tile_meta_stride
 // bytes, a multiple of 16) so that a warp copies it to shared memory in one go:
@@ -370,15 +371,25 @@ extern "C" int psx_tile_plan_fill(const int64_t* conn, int64_t E, int npe, int32
   std::vector<std::pair<int32_t, int32_t>> first;
   int32_t cap_p = 0, cap_n = 0;
   std::memset(meta, 0, (size_t)(n_tiles * M.stride));
-  // Group (key, code) entries of one tile: local indices in order of first occurrence,
-  // each group's codes ascending.  Writes codes to src and offsets to off.
+  // Group (key, code) entries of one tile: local indices by descending group size, ties
+  // in order of first occurrence, each group's codes ascending.  Writes codes to src and offsets to off.
   auto group = [&](uint8_t* src, uint8_t* off, std::vector<uint8_t>& map, int64_t e0, int per,
                    int shift) -> int32_t {
     std::sort(keys.begin(), keys.end());  // by key, then code
     first.clear();                         // (first code, start in keys)
     for (size_t k = 0; k < keys.size(); ++k)
       if (k == 0 || keys[k].first != keys[k - 1].first) first.push_back({keys[k].second, (int32_t)k});
-    std::sort(first.begin(), first.end());
+    // local numbering: most contributions first (ties by first occurrence), so that the
+    // 32 items a warp sums in one round have similar loop lengths
+    auto count = [&](const std::pair<int32_t, int32_t>& f) {
+      size_t k = (size_t)f.second;
+      while (k < keys.size() && keys[k].first == keys[(size_t)f.second].first) ++k;
+      return (int32_t)(k - (size_t)f.second);
+    };
+    std::sort(first.begin(), first.end(), [&](const auto& x, const auto& y) {
+      const int32_t cx = count(x), cy = count(y);
+      return cx != cy ? cx > cy : x.first < y.first;
+    });
     int32_t pos = 0, local = 0;
     for (const auto& f : first) {
       off[local] = (uint8_t)pos;

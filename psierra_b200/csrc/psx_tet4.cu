@@ -392,38 +392,52 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     // keeps the register count of the fused f + K tile low enough for 3 blocks per SM
     constexpr bool kTwoPass = PSX_TET4_TWO_PASS && !KGLOBAL && sizeof(KT) == 4 && !kLinear && !kMass;
     if constexpr (kTwoPass) {
-      float* fs = reinterpret_cast<float*>(krec);
+      // 44 floats as 11 16-byte accesses: with the 108-float slot stride the 8 lanes of
+      // each access phase fall on disjoint banks (scalar accesses put 4 lanes on a bank)
+      float v[44];
 #pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          fs[3 * b + k] = (float)p[b][k];
-          fs[12 + 3 * b + k] = (float)q[b][k];
-          fs[24 + 3 * b + k] = (float)gk[b][k];
+          v[3 * b + k] = (float)p[b][k];
+          v[12 + 3 * b + k] = (float)q[b][k];
+          v[24 + 3 * b + k] = (float)gk[b][k];
         }
-      fs[36] = (float)tc.A;
-      fs[37] = (float)tc.hb;
-      fs[38] = (float)tc.c;
-      fs[39] = (float)tc.phi;
-      fs[40] = (float)e_lam;
-      fs[41] = (float)e_mu;
-      fs[42] = (float)e_mass;
+      v[36] = (float)tc.A;
+      v[37] = (float)tc.hb;
+      v[38] = (float)tc.c;
+      v[39] = (float)tc.phi;
+      v[40] = (float)e_lam;
+      v[41] = (float)e_mu;
+      v[42] = (float)e_mass;
+      v[43] = 0.f;
+      float4* fs = reinterpret_cast<float4*>(krec);
+#pragma unroll
+      for (int i = 0; i < 11; ++i) fs[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
       asm volatile("" ::: "memory");
 #pragma unroll
+      for (int i = 0; i < 11; ++i) {
+        const float4 t = fs[i];
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+      }
+#pragma unroll
       for (int b = 0; b < 4; ++b)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          p[b][k] = (KT)fs[3 * b + k];
-          q[b][k] = (KT)fs[12 + 3 * b + k];
-          gk[b][k] = (KT)fs[24 + 3 * b + k];
+          p[b][k] = (KT)v[3 * b + k];
+          q[b][k] = (KT)v[12 + 3 * b + k];
+          gk[b][k] = (KT)v[24 + 3 * b + k];
         }
-      tc.A = (KT)fs[36];
-      tc.hb = (KT)fs[37];
-      tc.c = (KT)fs[38];
-      tc.phi = (KT)fs[39];
-      e_lam = (KT)fs[40];
-      e_mu = (KT)fs[41];
-      e_mass = (KT)fs[42];
+      tc.A = (KT)v[36];
+      tc.hb = (KT)v[37];
+      tc.c = (KT)v[38];
+      tc.phi = (KT)v[39];
+      e_lam = (KT)v[40];
+      e_mu = (KT)v[41];
+      e_mass = (KT)v[42];
     }
     KT w[4][3], h[4][3], y[4][3];
 #pragma unroll
@@ -472,8 +486,8 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
 //
 // Tile records (FP32 tangent, and every sweep without a tangent): the 32 elements of a
 // warp's tile stage their blocks and f triples in shared memory; the warp then sums the
-// blocks its elements share (psx_tile_plan_fill: local pairs / nodes in first-occurrence
-// order, contributions in element order) and writes one record per distinct pair and
+// blocks its elements share (psx_tile_plan_fill: local pairs / nodes by descending
+// contribution count, contributions in element order) and writes one record per distinct pair and
 // node, with consecutive lanes on consecutive records.  The FP64 tangent writes one
 // record per element straight to the ring.
 constexpr int kStageStride = RecLayout<4>::kK + 4;  // floats per staged element record (bank spread)
