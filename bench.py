@@ -593,9 +593,14 @@ def main():
             t = torch.tensor([msf], device=dev)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             msf = float(t.item())
+        # conn, X and u, the two-ring K values (FP64) and f: what the sweep must move
+        bytes_f = 16 * mf.n_elements + 48 * mf.n_nodes + 8 * af.nnz + 24 * mf.n_nodes
         fbar = {"workload": "cube 30^3 Kuhn Tet4Fbar (162,000 elements, 29,791 nodes), E=1e4 nu=0.49, "
                             "f_int + K_dev + K_vol on the two-ring pattern",
-                "ms": msf, "elements_per_s": world * mf.n_elements / (msf * 1e-3), "nnz_two_ring": af.nnz}
+                "ms": msf, "elements_per_s": world * mf.n_elements / (msf * 1e-3), "nnz_two_ring": af.nnz,
+                "algorithmic_bytes": bytes_f, "gbs": bytes_f / (msf * 1e-3) / 1e9,
+                "frac": bytes_f / (msf * 1e-3) / 1e9 / peak_hbm()[0],
+                "launches_per_call": 6}
         del af
 
     e2e = None

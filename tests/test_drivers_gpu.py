@@ -56,9 +56,10 @@ def test_newton_cube_matches_reference(key, n_steps, tol):
     assert list(r.iteration_history) == list(g[f"{key}_iterations"])
     trace = np.stack(dom.trace)
     assert trace.shape == g[f"{key}_trace"].shape
-    assert rel_max(trace, g[f"{key}_trace"]) < 1e-10
-    assert rel_2(r.displacement, g[f"{key}_u"]) < 1e-10
-    assert rel_max(r.reactions, g[f"{key}_reactions"]) < 1e-8
+    # measured: trace <= 9.4e-14, u <= 8.3e-14, reactions <= 3.0e-13
+    assert rel_max(trace, g[f"{key}_trace"]) < 1e-12
+    assert rel_2(r.displacement, g[f"{key}_u"]) < 1e-12
+    assert rel_max(r.reactions, g[f"{key}_reactions"]) < 1e-11
 
 
 def test_dynamic_relaxation_kinetic_cube_matches_reference():
@@ -70,8 +71,9 @@ def test_dynamic_relaxation_kinetic_cube_matches_reference():
     r = dr.solve(clamp_manager(cube, g["fz15_fixed"]), f_ext=g["fz15_f_ext"], tol=1e-4, max_steps=1000)
     assert r.converged
     assert r.steps_completed == int(g["dr_kinetic_steps"]) and r.kinetic_peaks == int(g["dr_kinetic_peaks"])
-    assert rel_2(r.displacement, g["dr_kinetic_u"]) < 1e-9
-    assert rel_max(np.array(r.residual_history), g["dr_kinetic_history"]) < 1e-8
+    # measured: u 6.5e-14, residual history 2.3e-12
+    assert rel_2(r.displacement, g["dr_kinetic_u"]) < 1e-12
+    assert rel_max(np.array(r.residual_history), g["dr_kinetic_history"]) < 1e-10
 
 
 @pytest.mark.parametrize("solver", ["direct", "gpu-cg"])
@@ -87,9 +89,9 @@ def test_newton_beam_matches_reference(solver):
     ref_u = g["u"] if solver == "direct" else g["cg_u"]
     ref_it = g["iterations"] if solver == "direct" else g["cg_iterations"]
     assert list(r.iteration_history) == list(ref_it)
-    assert rel_2(r.displacement, ref_u) < (1e-10 if solver == "direct" else 1e-8)
+    assert rel_2(r.displacement, ref_u) < 1e-12  # measured 3.4e-14 (direct), 3.2e-14 (GPU CG)
     if solver == "direct":
-        assert rel_max(np.stack(dom.trace), g["trace"]) < 1e-9
+        assert rel_max(np.stack(dom.trace), g["trace"]) < 1e-11  # measured 2.6e-13
 
 
 def test_dynamic_relaxation_viscous_beam_matches_reference():
@@ -100,8 +102,10 @@ def test_dynamic_relaxation_viscous_beam_matches_reference():
     dr = DynamicRelaxationAnalysis(dom, damping_type="viscous", viscous_damping=0.1, safety_factor=1.1, dt=1.0)
     r = dr.solve(clamp_manager(mb, g["clamp"]), f_ext=g["f_ext"], tol=1e-12, max_steps=400, min_steps=10)
     assert r.steps_completed == int(g["dr_viscous_steps"])
-    assert rel_2(r.displacement, g["dr_viscous_u"]) < 1e-9
-    assert rel_max(np.array(r.residual_history), g["dr_viscous_history"]) < 1e-8
+    # measured: u 1.5e-13, residual history 1.4e-11 (its late entries are residuals near the
+    # 1e-12 stopping tolerance, where the reference's own f_int rounding is a visible share)
+    assert rel_2(r.displacement, g["dr_viscous_u"]) < 1e-12
+    assert rel_max(np.array(r.residual_history), g["dr_viscous_history"]) < 5e-10
 
 
 def test_cfg1_first_newton_iterates_match_reference():
@@ -114,7 +118,9 @@ def test_cfg1_first_newton_iterates_match_reference():
     assert not r.converged and bool(g["converged"]) is False
     trace = np.stack(dom.trace)
     assert trace.shape == g["trace"].shape
-    assert rel_max(trace, g["trace"]) < 1e-8
+    # measured 4.3e-11: these iterates do not converge, and the tangent's condition number
+    # (~2e6) amplifies the reference's own O(mu) rounding of f_int (~1e-13 relative)
+    assert rel_max(trace, g["trace"]) < 1e-9
 
 
 def test_mass_matrix_matches_oracle():
