@@ -59,10 +59,11 @@ def internal_force(asm: GPUAssembler, X, u, mu_e, kappa_e):
 
 class StaticEquilibrium(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, mu_e, kappa_e, f_ext, newton: DeviceNewton, n_steps: int, nr_tol: float, polish: int):
+    def forward(ctx, mu_e, kappa_e, f_ext, newton: DeviceNewton, n_steps: int, nr_tol: float, polish: int, u0=None):
         asm = newton.asm
         _set_params(asm, None, mu_e, kappa_e)
-        res = newton.solve(f_ext.detach(), n_steps=n_steps, nr_tol=nr_tol, polish=polish)
+        res = newton.solve(f_ext.detach(), u0=None if u0 is None else u0.detach(), n_steps=n_steps, nr_tol=nr_tol,
+                           polish=polish)
         if not res.converged:
             raise RuntimeError("static equilibrium did not converge")
         ctx.newton = newton
@@ -78,13 +79,16 @@ class StaticEquilibrium(torch.autograd.Function):
         rhs = torch.where(nt.free, gu.detach(), torch.zeros_like(gu))
         lam, _ = nt.solve_linear(rhs)
         _, gmu, gk = nt.asm.adjoint(u, lam)
-        return -gmu, -gk, lam, None, None, None, None
+        return -gmu, -gk, lam, None, None, None, None, None
 
 
 def static_equilibrium(newton: DeviceNewton, mu_e, kappa_e, f_ext, n_steps: int = 1, nr_tol: float = 1e-10,
-                       polish: int = 2):
-    """u*(mu_e, kappa_e, f_ext) with an adjoint backward; ``polish`` as in ``DeviceNewton.solve``."""
-    return StaticEquilibrium.apply(mu_e, kappa_e, f_ext, newton, n_steps, nr_tol, polish)
+                       polish: int = 2, u0=None):
+    """u*(mu_e, kappa_e, f_ext) with an adjoint backward; ``polish`` as in ``DeviceNewton.solve``.
+
+    ``u0`` starts Newton from a nearby equilibrium (for instance that of slightly different
+    moduli) instead of from zero; it is not differentiated."""
+    return StaticEquilibrium.apply(mu_e, kappa_e, f_ext, newton, n_steps, nr_tol, polish, u0)
 
 
 def identify_shear_moduli(newton: DeviceNewton, f_ext, obs_dofs, u_target, mu0, kappa_ratio: float = 50.0,

@@ -185,28 +185,10 @@ __device__ __forceinline__ double spmv_row(int64_t n, int64_t row, int lane8, co
 // quarter warp per node: lane l takes neighbours l, l + 8, ...; it reads the neighbour's
 // column once (from row 3i), x once for the three rows, and the 3x3 block's values, then
 // the three sums are reduced over the lane group in a fixed order.
+// Scalar loads: the 8 lanes of a group read 24 consecutive values of a row per load
+// instruction.  Loading each row segment and x triple as an aligned pair plus a scalar
+// (9 instead of 13 loads per neighbour) measured slower: 0.194 instead of 0.155 ms.
 constexpr int kNodeLanes = 8;  // PCG iteration on the 3.07M-element cube: 0.157 ms (16 lanes 0.176, 4 lanes 0.165)
-
-// Three consecutive values in two loads: the pair that is aligned to twice the value
-// size and the remaining value, chosen by predicates (no divergence).  Row segments of
-// a 3x3 block are 4-byte aligned floats (or 8-byte doubles) and x triples start on 8
-// bytes, so a vector half always exists.
-__device__ __forceinline__ void load3(const float* p, float& a, float& b, float& c) {
-  const bool al = (reinterpret_cast<uintptr_t>(p) & 7) == 0;
-  const float2 v = *reinterpret_cast<const float2*>(al ? p : p + 1);
-  const float s = al ? p[2] : p[0];
-  a = al ? v.x : s;
-  b = al ? v.y : v.x;
-  c = al ? s : v.y;
-}
-__device__ __forceinline__ void load3(const double* p, double& a, double& b, double& c) {
-  const bool al = (reinterpret_cast<uintptr_t>(p) & 15) == 0;
-  const double2 v = __ldcg(reinterpret_cast<const double2*>(al ? p : p + 1));
-  const double s = __ldcg(al ? p + 2 : p);
-  a = al ? v.x : s;
-  b = al ? v.y : v.x;
-  c = al ? s : v.y;
-}
 template <typename VT>
 __device__ __forceinline__ void spmv_node(int64_t nodes, int64_t node, int lane16, const int32_t* __restrict__ indptr,
                                           const int32_t* __restrict__ indices, const VT* __restrict__ vals,
@@ -220,15 +202,13 @@ __device__ __forceinline__ void spmv_node(int64_t nodes, int64_t node, int lane1
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   for (int32_t b3 = 3 * lane16; b3 < len; b3 += 3 * kNodeLanes) {
     const int32_t c = indices[r0 + b3];
-    double x0, x1, x2;
-    load3(x + c, x0, x1, x2);
-    VT v[3][3];
-    load3(vals + r0 + b3, v[0][0], v[0][1], v[0][2]);
-    load3(vals + r0 + b3 + len, v[1][0], v[1][1], v[1][2]);
-    load3(vals + r0 + b3 + 2 * len, v[2][0], v[2][1], v[2][2]);
-    a0 += (double)v[0][0] * x0 + (double)v[0][1] * x1 + (double)v[0][2] * x2;
-    a1 += (double)v[1][0] * x0 + (double)v[1][1] * x1 + (double)v[1][2] * x2;
-    a2 += (double)v[2][0] * x0 + (double)v[2][1] * x1 + (double)v[2][2] * x2;
+    const double x0 = __ldcg(x + c), x1 = __ldcg(x + c + 1), x2 = __ldcg(x + c + 2);
+    const VT* v0 = vals + r0 + b3;
+    const VT* v1 = v0 + len;
+    const VT* v2 = v1 + len;
+    a0 += (double)v0[0] * x0 + (double)v0[1] * x1 + (double)v0[2] * x2;
+    a1 += (double)v1[0] * x0 + (double)v1[1] * x1 + (double)v1[2] * x2;
+    a2 += (double)v2[0] * x0 + (double)v2[1] * x1 + (double)v2[2] * x2;
   }
 #pragma unroll
   for (int o = kNodeLanes / 2; o > 0; o >>= 1) {

@@ -204,11 +204,12 @@ def dynamic_tet10_fixture():
                 M_data=M.data, M_indptr=M.indptr, M_indices=M.indices)
 
 
-def tet10_newton_fixture():
-    """The Tet10 cube solve at a reduced grid (3^3 cells -> 162 Tet10): clamp z = 0,
-    u_z = -0.2 prescribed on z = 1 and ramped over 8 increments (nonlinear_static.py:
-    271-272), E = 1e4, nu = 0.4, the reference's Newton with its direct solver."""
-    m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, 3, 3, 3))
+def tet10_newton_fixture(cells: int = 3, n_steps: int = 8, nr_iterations: int = 20):
+    """The Tet10 cube solve at a reduced grid (3^3 cells -> 162 Tet10 by default): clamp
+    z = 0, u_z = -0.2 prescribed on z = 1 and ramped over ``n_steps`` increments
+    (nonlinear_static.py:271-272), E = 1e4, nu = 0.4, the reference's Newton with its
+    direct solver."""
+    m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, cells, cells, cells))
     mat = nh(1e4, 0.4)
     bottom = meshgen.nodes_on_plane(m, 2, "min")
     top = meshgen.nodes_on_plane(m, 2, "max")
@@ -216,10 +217,18 @@ def tet10_newton_fixture():
     dm.add_constraint(DirichletConstraint(bottom, components=(0, 1, 2), value=0.0))
     dm.add_constraint(DirichletConstraint(top, components=(2,), value=-0.2))
     dom = SolidDomain(DuckMesh(m.nodes, m.elements), mat, Tet10TotalLagrangian(mat))
-    r = NonlinearStaticAnalysis(dom).solve(dirichlet=dm, f_ext=np.zeros(m.n_dofs), n_steps=8,
-                                           nr_iterations=20, nr_tol=1e-8, verbose=False)
+    r = NonlinearStaticAnalysis(dom).solve(dirichlet=dm, f_ext=np.zeros(m.n_dofs), n_steps=n_steps,
+                                           nr_iterations=nr_iterations, nr_tol=1e-8, verbose=False)
     return dict(u=r.displacement, converged=r.converged, iterations=np.array(r.iteration_history),
-                bottom=bottom, top=top, mu=mat.parameters.shear_modulus, kappa=mat.parameters.bulk_modulus)
+                bottom=bottom, top=top, mu=mat.parameters.shear_modulus, kappa=mat.parameters.bulk_modulus,
+                cells=cells, n_steps=n_steps)
+
+
+def tet10_compress6_fixture():
+    """The Tet10 compression workload's loading (20 increments of the top-face
+    displacement, 30 Newton iterations allowed, tolerance 1e-8) on 6^3 cells -> 1,296
+    Tet10: the reference's own Newton converges in 5 iterations per increment."""
+    return tet10_newton_fixture(cells=6, n_steps=20, nr_iterations=30)
 
 
 def main(only=None):
@@ -228,6 +237,7 @@ def main(only=None):
     if only:
         # fixtures that need no shared random stream can be regenerated on their own
         gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture, "tet10_newton": tet10_newton_fixture,
+                "tet10_compress6": tet10_compress6_fixture,
                 "dynamic_tet10": dynamic_tet10_fixture}
         for name in only:
             out[name] = gens[name]()
@@ -340,6 +350,7 @@ def main(only=None):
     out["fbar_box"] = fbar_fixture()
     out["dynamic_beam"] = dynamic_fixture()
     out["tet10_newton"] = tet10_newton_fixture()
+    out["tet10_compress6"] = tet10_compress6_fixture()
     out["dynamic_tet10"] = dynamic_tet10_fixture()
 
     for name, d in out.items():

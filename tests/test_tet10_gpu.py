@@ -139,3 +139,35 @@ def test_tet10_prescribed_compression_matches_reference_newton():
     assert res.converged and bool(g["converged"])
     assert res.iteration_history == g["iterations"].tolist()
     assert np.abs(res.u.cpu().numpy() - g["u"]).max() <= 1e-8 * np.abs(g["u"]).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32-mixed"])
+def test_tet10_compression_workload_loading_matches_reference_newton(precision):
+    """The Tet10 compression workload's loading (top face u_z = -0.2 over 20 increments,
+    Jacobi PCG, Newton tolerance 1e-8) on 6^3 cells -> 1,296 Tet10 through the device
+    Newton, against the reference's Newton with its direct solver
+    (analysis/nonlinear_static.py:250-404).  FP64: the same iteration counts and the
+    displacement within 1e-10; FP32-mixed tangent (the residual stays FP64, so Newton
+    still converges to the FP64 equilibrium): within 1e-8."""
+    import torch
+
+    from psierra_b200.assembler import GPUAssembler
+    from psierra_b200.newton import DeviceNewton
+
+    g = golden("tet10_compress6")
+    cells, n_steps = int(g["cells"]), int(g["n_steps"])
+    m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, cells, cells, cells))
+    E = m.n_elements
+    asm = GPUAssembler(m.nodes, m.elements, NeoHookeanField(np.full(E, float(g["mu"])), np.full(E, float(g["kappa"]))))
+    bottom, top = g["bottom"], g["top"]
+    fixed = np.concatenate([3 * bottom + c for c in range(3)] + [3 * top + 2])
+    up = np.zeros(m.n_dofs)
+    up[3 * top + 2] = -0.2
+    nt = DeviceNewton(asm, fixed, precision=precision, pcg_tol=1e-13, pcg_maxiter=100000, preconditioner="jacobi")
+    res = nt.solve(torch.zeros(m.n_dofs, dtype=torch.float64, device="cuda"),
+                   u_prescribed=torch.from_numpy(up).cuda(), n_steps=n_steps, nr_iterations=30, nr_tol=1e-8)
+    assert res.converged and bool(g["converged"])
+    if precision == "fp64":
+        assert res.iteration_history == g["iterations"].tolist()
+    tol = 1e-10 if precision == "fp64" else 1e-8
+    assert np.abs(res.u.cpu().numpy() - g["u"]).max() <= tol * np.abs(g["u"]).max()
