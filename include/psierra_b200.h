@@ -197,7 +197,8 @@ int psx_tet4_split_ready(void);
  * memory and writes one record per distinct pair / node.  Inputs: conn (E x 4), the
  * element-code item lists of psx_plan_fill.  Outputs (host buffers, n_tiles =
  * ceil(E / tile)): meta (n_tiles x psx_tile_meta_stride(tile) bytes; per tile: pair and
- * node counts, offsets and codes, laid out as psx_pattern.cpp describes), pair_ptr_t
+ * node counts, then the node offsets and codes, then the pair offsets and codes, laid
+ * out as psx_pattern.cpp describes), pair_ptr_t
  * (n_pairs + 1), pair_src_t (<= len pair_src), node_ptr_t (N + 1), node_src_t (<= len
  * node_src), caps[2] = {most pairs, most nodes in a tile}.  Contributions keep
  * ascending element order inside a tile and ascending tile order across tiles (a

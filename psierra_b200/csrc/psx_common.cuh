@@ -31,28 +31,49 @@ struct Mat3 {
   double m[3][3];
 };
 
+// Explicitly rounded arithmetic for the element math.  Every multiply, add and fused
+// multiply-add of the force and tangent is written out, so the compiler cannot fuse or
+// reorder them differently in different kernels: the warp-specialised kernel, the mixed
+// kernel and the effective-tangent kernel then compute the same bits for the same
+// element (a schedule change never changes a result).
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// a b - c d with c d rounded once
+__device__ __forceinline__ double dmm(double a, double b, double c, double d) { return dfma(a, b, -dmul(c, d)); }
+// a0 b0 + a1 b1 + a2 b2, accumulated from the last term
+__device__ __forceinline__ double ddot3(double a0, double b0, double a1, double b1, double a2, double b2) {
+  return dfma(a0, b0, dfma(a1, b1, dmul(a2, b2)));
+}
+__device__ __forceinline__ float fdot3(float a0, float b0, float a1, float b1, float a2, float b2) {
+  return ffma(a0, b0, ffma(a1, b1, fmul(a2, b2)));
+}
+
 __device__ __forceinline__ double det3(const double a[3][3]) {
-  return a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
-         a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
-         a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+  return ddot3(a[0][0], dmm(a[1][1], a[2][2], a[1][2], a[2][1]), a[0][1], dmm(a[1][2], a[2][0], a[1][0], a[2][2]),
+               a[0][2], dmm(a[1][0], a[2][1], a[1][1], a[2][0]));
 }
 
 // Inverse through the adjugate; returns the determinant.
 __device__ __forceinline__ double inv3(const double a[3][3], double r[3][3]) {
-  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
-  double c01 = a[0][2] * a[2][1] - a[0][1] * a[2][2];
-  double c02 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
-  double c10 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
-  double c11 = a[0][0] * a[2][2] - a[0][2] * a[2][0];
-  double c12 = a[0][2] * a[1][0] - a[0][0] * a[1][2];
-  double c20 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
-  double c21 = a[0][1] * a[2][0] - a[0][0] * a[2][1];
-  double c22 = a[0][0] * a[1][1] - a[0][1] * a[1][0];
-  double det = a[0][0] * c00 + a[0][1] * c10 + a[0][2] * c20;
-  double id = 1.0 / det;
-  r[0][0] = c00 * id; r[0][1] = c01 * id; r[0][2] = c02 * id;
-  r[1][0] = c10 * id; r[1][1] = c11 * id; r[1][2] = c12 * id;
-  r[2][0] = c20 * id; r[2][1] = c21 * id; r[2][2] = c22 * id;
+  const double c00 = dmm(a[1][1], a[2][2], a[1][2], a[2][1]);
+  const double c01 = dmm(a[0][2], a[2][1], a[0][1], a[2][2]);
+  const double c02 = dmm(a[0][1], a[1][2], a[0][2], a[1][1]);
+  const double c10 = dmm(a[1][2], a[2][0], a[1][0], a[2][2]);
+  const double c11 = dmm(a[0][0], a[2][2], a[0][2], a[2][0]);
+  const double c12 = dmm(a[0][2], a[1][0], a[0][0], a[1][2]);
+  const double c20 = dmm(a[1][0], a[2][1], a[1][1], a[2][0]);
+  const double c21 = dmm(a[0][1], a[2][0], a[0][0], a[2][1]);
+  const double c22 = dmm(a[0][0], a[1][1], a[0][1], a[1][0]);
+  const double det = ddot3(a[0][0], c00, a[0][1], c10, a[0][2], c20);
+  const double id = 1.0 / det;
+  r[0][0] = dmul(c00, id); r[0][1] = dmul(c01, id); r[0][2] = dmul(c02, id);
+  r[1][0] = dmul(c10, id); r[1][1] = dmul(c11, id); r[1][2] = dmul(c12, id);
+  r[2][0] = dmul(c20, id); r[2][1] = dmul(c21, id); r[2][2] = dmul(c22, id);
   return det;
 }
 
@@ -72,21 +93,22 @@ struct PointState {
 // neohookean.py:74-92 restated without cancellation (see the header comment).
 __device__ __forceinline__ void neohookean_point(const double l[3][3], double mu, double kappa,
                                                  PointState& s) {
-  double trl = l[0][0] + l[1][1] + l[2][2];
-  double trl2 = 0.0;
+  const double trl = dadd(dadd(l[0][0], l[1][1]), l[2][2]);
+  double trl2 = dmul(l[0][0], l[0][0]);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) trl2 += l[i][k] * l[k][i];
-  s.Jm1 = trl + 0.5 * (trl * trl - trl2) + det3(l);
+    for (int k = 0; k < 3; ++k)
+      if (i + k > 0) trl2 = dfma(l[i][k], l[k][i], trl2);
+  s.Jm1 = dadd(dadd(trl, dmul(0.5, dfma(trl, trl, -trl2))), det3(l));
   const double lnJ = log1p(s.Jm1);
   s.lnJ = lnJ;
-  s.phi = mu * exp((-2.0 / 3.0) * lnJ);
-  s.beta = kappa * lnJ;
+  s.phi = dmul(mu, exp(dmul(-2.0 / 3.0, lnJ)));
+  s.beta = dmul(kappa, lnJ);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) s.F[i][j] = (i == j ? 1.0 : 0.0) + l[i][j];
+    for (int j = 0; j < 3; ++j) s.F[i][j] = i == j ? dadd(1.0, l[i][j]) : l[i][j];
   inv3(s.F, s.Finv);
   // Green-Lagrange strain E = (l + l^T + l^T l) / 2 (symmetric: six entries formed)
   double E[3][3];
@@ -94,20 +116,20 @@ __device__ __forceinline__ void neohookean_point(const double l[3][3], double mu
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = i; j < 3; ++j) {
-      double ltl = l[0][i] * l[0][j] + l[1][i] * l[1][j] + l[2][i] * l[2][j];
-      E[i][j] = 0.5 * (l[i][j] + l[j][i] + ltl);
+      const double ltl = ddot3(l[0][i], l[0][j], l[1][i], l[1][j], l[2][i], l[2][j]);
+      E[i][j] = dmul(0.5, dadd(dadd(l[i][j], l[j][i]), ltl));
       E[j][i] = E[i][j];
     }
-  double trE = E[0][0] + E[1][1] + E[2][2];
-  s.I1 = 3.0 + 2.0 * trE;
+  const double trE = dadd(dadd(E[0][0], E[1][1]), E[2][2]);
+  s.I1 = dfma(2.0, trE, 3.0);
   // T = 2 phi dev E + beta I (symmetric)
   double T[3][3];
-  const double tw = 2.0 * s.phi, dia = s.beta - tw * (trE / 3.0);
+  const double tw = dmul(2.0, s.phi), dia = dfma(-tw, trE / 3.0, s.beta);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = i; j < 3; ++j) {
-      T[i][j] = tw * E[i][j] + (i == j ? dia : 0.0);
+      T[i][j] = i == j ? dfma(tw, E[i][j], dia) : dmul(tw, E[i][j]);
       T[j][i] = T[i][j];
     }
   // S = C^-1 T, so P = F S = F F^-1 F^-T T = F^-T T: the first Piola stress without
@@ -116,7 +138,7 @@ __device__ __forceinline__ void neohookean_point(const double l[3][3], double mu
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j)
-      s.P[i][j] = s.Finv[0][i] * T[0][j] + s.Finv[1][i] * T[1][j] + s.Finv[2][i] * T[2][j];
+      s.P[i][j] = ddot3(s.Finv[0][i], T[0][j], s.Finv[1][i], T[1][j], s.Finv[2][i], T[2][j]);
 }
 
 // Tangent coefficients with the integration weight folded in.
@@ -128,10 +150,10 @@ struct TangentCoef {
 template <typename T>
 __device__ __forceinline__ TangentCoef<T> tangent_coef(const PointState& s, double kappa, double w) {
   TangentCoef<T> t;
-  t.A = (T)(w * (kappa + (2.0 / 9.0) * s.phi * s.I1));
-  t.hb = (T)(w * (s.phi * s.I1 / 3.0 - s.beta));
-  t.c = (T)(w * (-(2.0 / 3.0) * s.phi));
-  t.phi = (T)(w * s.phi);
+  t.A = (T)dmul(w, dfma(dmul(2.0 / 9.0, s.phi), s.I1, kappa));
+  t.hb = (T)dmul(w, dsub(dmul(s.phi, s.I1) / 3.0, s.beta));
+  t.c = (T)dmul(w, dmul(-2.0 / 3.0, s.phi));
+  t.phi = (T)dmul(w, s.phi);
   return t;
 }
 

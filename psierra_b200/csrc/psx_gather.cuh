@@ -52,10 +52,11 @@ struct GatherArgs {
   int32_t cap_p4, cap_n4;
   int32_t tile_k;             // K values per tile record: 9 cap_p4 + 6 cap_n4
   // per-tile reduction lists (psx_tile_plan_fill): one block of meta_stride bytes per
-  // tile, fields at byte offsets off_p (pair offsets), off_n (node offsets), src_p (pair
-  // codes), src_n (node codes); byte 0 / 1 = pair / node count
+  // tile, fields at byte offsets off_n (node offsets), src_n (node codes), off_p (pair
+  // offsets), src_p (pair codes); byte 0 / 1 = pair / node count.  The first
+  // meta_node_bytes hold the count bytes and the node lists.
   const uint8_t* tile_meta;
-  int32_t meta_stride, off_p, off_n, src_p, src_n;
+  int32_t meta_stride, meta_node_bytes, off_p, off_n, src_p, src_n;
   int32_t tile;
 };
 
@@ -149,16 +150,33 @@ struct NodeBatch {
   static constexpr int n = sizeof(KT) == 8 ? 2 : (NPE == 4 && WANT_K && WANT_F ? 1 : 4);
 };
 
+// What a gather item starts from: its output positions (pair_info / node_info) and the
+// bounds of its contribution list.  The warp-specialised gather loads it for its next
+// task while the current one runs.
+struct ItemHead {
+  int4 info;
+  int32_t s0, s1;
+};
+template <bool TILES>
+__device__ __forceinline__ ItemHead pair_head(const GatherArgs& g, int32_t p) {
+  const int32_t* lptr = TILES ? g.pair_ptr_t : g.pair_ptr;
+  return ItemHead{__ldg(reinterpret_cast<const int4*>(g.pair_info) + p), __ldg(lptr + p), __ldg(lptr + p + 1)};
+}
+template <bool TILES>
+__device__ __forceinline__ ItemHead node_head(const GatherArgs& g, int32_t n) {
+  const int32_t* lptr = TILES ? g.node_ptr_t : g.node_ptr;
+  return ItemHead{__ldg(reinterpret_cast<const int4*>(g.node_info) + n), __ldg(lptr + n), __ldg(lptr + n + 1)};
+}
+
 // Pair item: off-diagonal block and its transpose.  Contributions are summed in list
 // (ascending element) order; their loads are issued kBatch at a time.
 template <typename KT, int NPE, bool TILES = false, bool WANT_F = false, int BATCH = 0, bool VSTORE = false>
-__device__ __forceinline__ void gather_pair(const GatherArgs& g, int32_t p, const KT* __restrict__ krec,
+__device__ __forceinline__ void gather_pair(const GatherArgs& g, const ItemHead& h, const KT* __restrict__ krec,
                                             KT* __restrict__ k_out) {
   using L = RecLayout<NPE>;
-  const int4 info = __ldg(reinterpret_cast<const int4*>(g.pair_info) + p);
+  const int4 info = h.info;
   const int32_t* list = TILES ? g.pair_src_t : g.pair_src;
-  const int32_t* lptr = TILES ? g.pair_ptr_t : g.pair_ptr;
-  const int32_t s0 = __ldg(lptr + p), s1 = __ldg(lptr + p + 1);
+  const int32_t s0 = h.s0, s1 = h.s1;
   KT acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = (KT)0;
@@ -224,14 +242,13 @@ struct DRArgs {
 // Node item: diagonal block and/or f (or, with DR, the fused pseudo-step on f = K x).
 template <typename KT, int NPE, bool WANT_K, bool WANT_F, bool DR = false, bool TILES = false, int BATCH = 0,
           bool VSTORE = false>
-__device__ __forceinline__ void gather_node(const GatherArgs& g, int32_t n, const KT* __restrict__ krec,
+__device__ __forceinline__ void gather_node(const GatherArgs& g, const ItemHead& h, const KT* __restrict__ krec,
                                             const double* __restrict__ frec, KT* __restrict__ k_out,
                                             double* __restrict__ f_out, const DRArgs* dr = nullptr) {
   using L = RecLayout<NPE>;
-  const int4 info = __ldg(reinterpret_cast<const int4*>(g.node_info) + n);
+  const int4 info = h.info;
   const int32_t* list = TILES ? g.node_src_t : g.node_src;
-  const int32_t* lptr = TILES ? g.node_ptr_t : g.node_ptr;
-  const int32_t s0 = __ldg(lptr + n), s1 = __ldg(lptr + n + 1);
+  const int32_t s0 = h.s0, s1 = h.s1;
   KT acc[6];
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc[j] = (KT)0;
@@ -394,31 +411,35 @@ __device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
   return v;
 }
 
-// Bounded wait, executed by a whole warp: lane j checks counter[first + j] >=
-// target(first + j) for j < count.  Returns false (and flags the status) if the wait
-// gives up; the caller then still proceeds, so every access stays in bounds and the
-// host reports the failure.
+// Bounded wait on a prefix, executed by a whole warp: returns once every granule
+// g <= need has reached target(g).  `done` is the warp's watermark (every granule
+// <= done is known complete; start at -1): a wait below it costs nothing, and each poll
+// reads the 32 counters after it in one load and advances it over their complete run,
+// so one poll usually covers the warp's next few tasks.  A prefix implies the spans the
+// queue needs (an element tile: the gathers of the granules its ring slots held; a
+// gather: the element tiles of its span), and everything it adds was claimed earlier in
+// the same in-order lists, so the queue still drains.  After `max_spins` polls (or
+// once another wait has given up) it sets status flag bit 0 and returns false; the
+// caller still proceeds, so every access stays in bounds and the host reports it.
 template <typename Target>
-__device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first, int32_t count, Target target,
-                                              Status* st, int32_t max_spins) {
+__device__ __forceinline__ bool wait_prefix(const int32_t* cnt, int32_t need, int32_t n, Target target, int32_t& done,
+                                            Status* st, int32_t max_spins) {
+  if (need <= done) return true;
   const int lane = threadIdx.x & 31;
-  for (int32_t base = 0; base < count; base += 32) {
-    const int32_t g = first + base + lane;
-    const bool mine = (base + lane) < count && g >= 0;
-    const int32_t want = mine ? target(g) : 0;
-    int spins = 0;
-    while (true) {
-      const bool ok = !mine || ld_acquire(cnt + g) >= want;
-      if (__all_sync(0xffffffffu, ok)) break;
-      // once any wait has given up, every later wait returns at once
-      if (++spins > max_spins || (ld_acquire(&st->flags) & 1)) {
-        if (lane == 0) atomicOr(&st->flags, 1);
-        return false;
-      }
-      if (spins > 64) __nanosleep(200);
+  int spins = 0;
+  while (true) {
+    const int32_t g = done + 1 + lane;
+    const bool ok = g >= n || ld_acquire(cnt + g) >= target(g);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    done += m == 0xffffffffu ? 32 : __ffs(~m) - 1;
+    if (need <= done) break;
+    if (++spins > max_spins || (ld_acquire(&st->flags) & 1)) {
+      if (lane == 0) atomicOr(&st->flags, 1);
+      return false;
     }
-    if (spins && lane == 0) atomicAdd(&st->iters, spins);
+    if (spins > 64) __nanosleep(200);
   }
+  if (spins && lane == 0) atomicAdd(&st->iters, spins);
   return true;
 }
 
@@ -443,6 +464,7 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
     return (int32_t)((n + Q.tile - 1) / Q.tile);
   };
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
+  int32_t evaluated = -1, gathered = -1;  // watermarks of wait_prefix
   int32_t next = 0;
   if (lane == 0) next = atomicAdd(Q.counters, 1);
   while (true) {
@@ -453,7 +475,8 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
     const int32_t gr = task.y;
     if (task.x == 0) {
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st, Q.max_spins);
+      if (old >= 0)
+        wait_prefix(bcnt, min(old + Q.span_g + 1, Q.n_granules - 1), Q.n_granules, btiles, gathered, st, Q.max_spins);
       __syncwarp();
       element_tile(task);
       __syncwarp();
@@ -462,16 +485,16 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
         atomicAdd(acnt + gr, 1);
       }
     } else {
-      const int32_t first = max(0, gr - Q.span_g - 1);
-      wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
+      wait_prefix(acnt, gr, Q.n_granules, atiles, evaluated, st, Q.max_spins);
       __syncwarp();
       for (int32_t item = task.z + lane; item < task.w; item += 32) {
         // K row segments leave as vector + scalar pairs (FP64 f+K 2.35 -> 2.26 ms, Tet10
         // 0.70 / 1.10 -> 0.66 / 1.05 ms on the benchmark meshes)
         if (task.x == 1) {
-          if constexpr (WANT_K) gather_pair<KT, NPE, TILES, WANT_F, 0, true>(g, item, krec, k_out);
+          if constexpr (WANT_K) gather_pair<KT, NPE, TILES, WANT_F, 0, true>(g, pair_head<TILES>(g, item), krec, k_out);
         } else {
-          gather_node<KT, NPE, WANT_K, WANT_F, DR, TILES, 0, true>(g, item, krec, frec, k_out, f_out, &dr);
+          gather_node<KT, NPE, WANT_K, WANT_F, DR, TILES, 0, true>(g, node_head<TILES>(g, item), krec, frec, k_out,
+                                                                    f_out, &dr);
         }
       }
       __syncwarp();
@@ -489,30 +512,71 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
 // task waits only on tasks claimed before it (claims are in order in both lists), so the
 // loops cannot deadlock while the warps that claimed tasks are resident; a wait that
 // gives up flags the status and the task proceeds in bounds.
+// Tuning switches of the warp-specialised loops: load the next element tile's
+// connectivity / the next gather task's item heads while the current one runs.
+#ifndef PSX_SPLIT_PREFETCH_CONN
+#define PSX_SPLIT_PREFETCH_CONN 1
+#endif
+#ifndef PSX_SPLIT_PREFETCH_HEADS
+#define PSX_SPLIT_PREFETCH_HEADS 1
+#endif
+
 template <typename ElementTile>
-__device__ __forceinline__ void drain_elements(const QueueArgs& Q, int32_t* ecnt, Status* st,
-                                               ElementTile&& element_tile) {
+__device__ __forceinline__ void drain_elements(const QueueArgs& Q, const int4* __restrict__ conn, int32_t* ecnt,
+                                               Status* st, ElementTile&& element_tile) {
   const int lane = threadIdx.x & 31;
   int32_t* acnt = Q.counters + 1;
   int32_t* bcnt = Q.counters + 1 + Q.n_granules;
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
   const int64_t n_tiles = (Q.n_elements + Q.tile - 1) / Q.tile;
-  int32_t next = 0;
-  if (lane == 0) next = atomicAdd(ecnt, 1);
-  while (true) {
-    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
-    if (t >= n_tiles) break;
-    if (lane == 0) next = atomicAdd(ecnt, 1);
+  int32_t gathered = -1;  // watermark: the gathers of every granule <= gathered are done
+  // A finished tile is published during the warp's next tile, after that tile's
+  // evaluation: the release then finds the tile's record stores long completed instead
+  // of waiting for them (relaxed adds in place of the release measured 9% faster).  The
+  // warp publishes before any wait that could block, so it never waits while holding an
+  // unpublished tile and the queue drains as before.
+  int32_t pending = -1;
+  auto publish_pending = [&]() {
+    if (pending >= 0 && lane == 0) publish_tile(acnt + pending);
+    pending = -1;
+  };
+  // Tiles are claimed two ahead, so that the next tile's connectivity is loaded while
+  // the current one is evaluated (its node loads then start one memory round trip
+  // earlier).  A claimed tile waits only on earlier work, like every other task.
+  auto conn_of = [&](int32_t t) -> int4 {
+    const int64_t e = (int64_t)t * Q.tile + lane;
+    return (t < n_tiles && e < Q.n_elements) ? __ldg(conn + e) : make_int4(0, 0, 0, 0);
+  };
+  constexpr bool kPre = PSX_SPLIT_PREFETCH_CONN != 0;
+  int32_t claim = 0;
+  if (lane == 0) claim = atomicAdd(ecnt, 1);
+  int32_t t = __shfl_sync(0xffffffffu, claim, 0);
+  if (lane == 0 && t < n_tiles) claim = atomicAdd(ecnt, 1);
+  int4 cn = kPre ? conn_of(t) : make_int4(0, 0, 0, 0);
+  while (t < n_tiles) {
+    const int32_t tn = __shfl_sync(0xffffffffu, claim, 0);
+    if (lane == 0 && tn < n_tiles) claim = atomicAdd(ecnt, 1);
+    const int4 cn_next = kPre ? conn_of(tn) : make_int4(0, 0, 0, 0);
+    if constexpr (!kPre) cn = conn_of(t);
     const int64_t e0 = (int64_t)t * Q.tile;
     const int64_t e1 = min(e0 + (int64_t)Q.tile, Q.n_elements);
     const int32_t gr = (int32_t)(e0 >> Q.granule_log2);
     const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-    if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st, Q.max_spins);
+    if (old >= 0) {
+      const int32_t need = min(old + Q.span_g + 1, Q.n_granules - 1);
+      if (need > gathered) publish_pending();
+      wait_prefix(bcnt, need, Q.n_granules, btiles, gathered, st, Q.max_spins);
+    }
     __syncwarp();
-    element_tile(make_int4(0, gr, (int32_t)e0, (int32_t)e1));
+    element_tile(make_int4(0, gr, (int32_t)e0, (int32_t)e1), cn, publish_pending);
     __syncwarp();
-    if (lane == 0) publish_tile(acnt + gr);
+    publish_pending();  // no-op unless the tile did not publish its predecessor
+    pending = gr;
+    t = tn;
+    cn = cn_next;
   }
+  __syncwarp();
+  publish_pending();
 }
 
 template <typename KT, int NPE, bool WANT_K, bool WANT_F, int PAIR_BATCH, int NODE_BATCH>
@@ -528,29 +592,57 @@ __device__ __forceinline__ void drain_gathers(const GatherArgs& g, const QueueAr
     const int64_t n = min(gsize, Q.n_elements - (int64_t)r * gsize);
     return (int32_t)((n + Q.tile - 1) / Q.tile);
   };
-  int32_t next = 0;
-  if (lane == 0) next = atomicAdd(gcnt, 1);
-  while (true) {
-    const int32_t t = __shfl_sync(0xffffffffu, next, 0);
-    if (t >= n_gtasks) break;
-    if (lane == 0) next = atomicAdd(gcnt, 1);
-    const int4 task = __ldg(gtasks + t);
+  int32_t evaluated = -1;  // watermark: the element tiles of every granule <= evaluated are done
+  // Tasks are claimed two ahead: the next task and the heads of its items (output
+  // positions and list bounds, plan data that no wait guards) are loaded while the
+  // current task runs, which takes one memory round trip off each task's chain.
+  constexpr bool kPre = PSX_SPLIT_PREFETCH_HEADS != 0;
+  auto head_of = [&](const int4& task) -> ItemHead {
+    const int32_t item = task.z + lane;
+    if (item >= task.w) return ItemHead{make_int4(0, 0, 0, 0), 0, 0};
+    return task.x == 1 ? pair_head<true>(g, item) : node_head<true>(g, item);
+  };
+  int32_t claim = 0;
+  if (lane == 0) claim = atomicAdd(gcnt, 1);
+  int32_t t = __shfl_sync(0xffffffffu, claim, 0);
+  if (lane == 0 && t < n_gtasks) claim = atomicAdd(gcnt, 1);
+  int4 task = make_int4(0, 0, 0, 0);
+  ItemHead head{make_int4(0, 0, 0, 0), 0, 0};
+  if (t < n_gtasks) {
+    task = __ldg(gtasks + t);
+    if constexpr (kPre) head = head_of(task);
+  }
+  while (t < n_gtasks) {
+    const int32_t tn = __shfl_sync(0xffffffffu, claim, 0);
+    if (lane == 0 && tn < n_gtasks) claim = atomicAdd(gcnt, 1);
+    int4 task_n = make_int4(0, 0, 0, 0);
+    ItemHead head_n{make_int4(0, 0, 0, 0), 0, 0};
+    if (tn < n_gtasks) {
+      task_n = __ldg(gtasks + tn);
+      if constexpr (kPre) head_n = head_of(task_n);
+    }
     const int32_t gr = task.y;
-    const int32_t first = max(0, gr - Q.span_g - 1);
-    wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
+    wait_prefix(acnt, gr, Q.n_granules, atiles, evaluated, st, Q.max_spins);
     __syncwarp();
     // K values leave in float2 + float pairs per row segment: 12 instead of 18 store
     // instructions per pair block (f+K 0.76 -> 0.72 ms, K-only 0.69 -> 0.64 ms on the
     // 3.07M-element cube; the memory pipeline the two roles share is the bottleneck)
     for (int32_t item = task.z + lane; item < task.w; item += 32) {
+      // a task's first 32 items use the preloaded heads
+      const bool pre = kPre && item < task.z + 32;
       if (task.x == 1) {
-        if constexpr (WANT_K) gather_pair<KT, NPE, true, WANT_F, PAIR_BATCH, true>(g, item, krec, k_out);
+        if constexpr (WANT_K)
+          gather_pair<KT, NPE, true, WANT_F, PAIR_BATCH, true>(g, pre ? head : pair_head<true>(g, item), krec, k_out);
       } else {
-        gather_node<KT, NPE, WANT_K, WANT_F, false, true, NODE_BATCH, true>(g, item, krec, frec, k_out, f_out);
+        gather_node<KT, NPE, WANT_K, WANT_F, false, true, NODE_BATCH, true>(
+            g, pre ? head : node_head<true>(g, item), krec, frec, k_out, f_out);
       }
     }
     __syncwarp();
     if (lane == 0) atomicAdd(bcnt + gr, 1);
+    t = tn;
+    task = task_n;
+    head = head_n;
   }
 }
 
@@ -578,11 +670,12 @@ inline GatherArgs gather_args(const psx_plan_t* P, int64_t ring_elems) {
   {
     const int32_t T = P->tile > 0 ? P->tile : 1;
     auto up4 = [](int32_t b) { return (b + 3) / 4 * 4; };
-    g.off_p = 4;
-    g.off_n = g.off_p + up4(6 * T + 1);
-    g.src_p = g.off_n + up4(4 * T + 1);
-    g.src_n = g.src_p + 6 * T;
-    g.meta_stride = (g.src_n + 4 * T + 15) / 16 * 16;
+    g.off_n = 4;
+    g.src_n = g.off_n + up4(4 * T + 1);
+    g.off_p = g.src_n + 4 * T;
+    g.src_p = g.off_p + up4(6 * T + 1);
+    g.meta_stride = (g.src_p + 6 * T + 15) / 16 * 16;
+    g.meta_node_bytes = (g.off_p + 15) / 16 * 16;  // header and node lists
   }
   g.ring_tile_mask = P->tile > 0 ? ring_elems / P->tile - 1 : 0;
   return g;

@@ -330,10 +330,11 @@ extern "C" int psx_plan_fill(const int64_t* conn, int64_t E, int npe, int64_t N,
 // order.  Everything one tile needs is one contiguous block (psx_tile_meta_stride
 // bytes, a multiple of 16) so that a warp copies it to shared memory in one go:
 //   [0] np  [1] nn  [2..3] 0
-//   pair offsets  (np + 1 bytes, in a 4-byte-rounded field of 6T + 1)
 //   node offsets  (nn + 1 bytes, in a 4-byte-rounded field of 4T + 1)
-//   pair codes    (6T bytes, by local pair, element order within a pair)
 //   node codes    (4T bytes, element-in-tile * 4 + local node)
+//   pair offsets  (np + 1 bytes, in a 4-byte-rounded field of 6T + 1)
+//   pair codes    (6T bytes, by local pair, element order within a pair)
+// The node lists come first: the sweeps without a tangent copy only that prefix.
 // The gather lists then name (tile, local index) records instead of element slots, and
 // consecutive contributions of one tile collapse into one.
 namespace {
@@ -341,11 +342,11 @@ inline int64_t up4(int64_t b) { return (b + 3) / 4 * 4; }
 struct TileMeta {
   int64_t off_p, off_n, src_p, src_n, stride;
   explicit TileMeta(int64_t T) {
-    off_p = 4;
-    off_n = off_p + up4(6 * T + 1);
-    src_p = off_n + up4(4 * T + 1);
-    src_n = src_p + 6 * T;
-    stride = (src_n + 4 * T + 15) / 16 * 16;
+    off_n = 4;
+    src_n = off_n + up4(4 * T + 1);
+    off_p = src_n + 4 * T;
+    src_p = off_p + up4(6 * T + 1);
+    stride = (src_p + 6 * T + 15) / 16 * 16;
   }
 };
 }  // namespace

@@ -119,8 +119,21 @@ __device__ __forceinline__ void put_diag(KT* __restrict__ krec, int o, const KT 
   }
 }
 
+// Explicitly rounded operations in the tangent's type (dmul / fmul etc. of psx_common.cuh).
+__device__ __forceinline__ double xmul(double a, double b) { return dmul(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return fmul(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return dadd(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return fadd(a, b); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return dfma(a, b, c); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return ffma(a, b, c); }
+template <typename T>
+__device__ __forceinline__ T xdot3(T a0, T b0, T a1, T b1, T a2, T b2) {
+  return xfma(a0, b0, xfma(a1, b1, xmul(a2, b2)));
+}
+
+// `cn` = the element's connectivity (loaded by the caller, possibly ahead of time).
 template <typename KT, int MODE, bool KGLOBAL = true, bool FGLOBAL = true>
-__device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* __restrict__ krec,
+__device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, const int4 cn, KT* __restrict__ krec,
                                              double* __restrict__ frec) {
   using L = RecLayout<4>;
   constexpr bool kAdj = (MODE & kModeAdjoint) != 0;
@@ -129,7 +142,6 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
   constexpr bool kLinear = (MODE & PSX_LINEAR) != 0;
   constexpr bool kMass = (MODE & PSX_MASS) != 0;
   constexpr bool kWantK = ((MODE & PSX_WANT_K) != 0 || kLinear) && !kKV;
-  const int4 cn = __ldg(reinterpret_cast<const int4*>(A.conn) + e);
   double Xn[4][3];
   load_nodes(A.X, cn, Xn);
   // sweeps forming a tangent or K.v load the displacements with the coordinates (one
@@ -202,7 +214,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-          fr[3 * a + i] = G.V * (ps.P[i][0] * G.g[a][0] + ps.P[i][1] * G.g[a][1] + ps.P[i][2] * G.g[a][2]);
+          fr[3 * a + i] = dmul(G.V, ddot3(ps.P[i][0], G.g[a][0], ps.P[i][1], G.g[a][1], ps.P[i][2], G.g[a][2]));
       store_f12<FGLOBAL>(frec, fr, A.plane);
     }
     if constexpr (kWantK || kKV) {
@@ -219,8 +231,8 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
       for (int b = 0; b < 4; ++b)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          p[b][k] = Fi[0][k] * gk[b][0] + Fi[1][k] * gk[b][1] + Fi[2][k] * gk[b][2];
-          q[b][k] = Fm[k][0] * gk[b][0] + Fm[k][1] * gk[b][1] + Fm[k][2] * gk[b][2];
+          p[b][k] = xdot3(Fi[0][k], gk[b][0], Fi[1][k], gk[b][1], Fi[2][k], gk[b][2]);
+          q[b][k] = xdot3(Fm[k][0], gk[b][0], Fm[k][1], gk[b][1], Fm[k][2], gk[b][2]);
         }
     }
   }
@@ -251,12 +263,12 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     for (int b = 0; b < 4; ++b) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        alpha += (tc.A * p[b][k] + tc.c * q[b][k]) * vk[b][k];
-        beta += p[b][k] * vk[b][k];
+        alpha = xfma(xfma(tc.A, p[b][k], xmul(tc.c, q[b][k])), vk[b][k], alpha);
+        beta = xfma(p[b][k], vk[b][k], beta);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          Pv[k][m] += p[b][k] * vk[b][m];
-          Gv[k][m] += gk[b][k] * vk[b][m];
+          Pv[k][m] = xfma(p[b][k], vk[b][m], Pv[k][m]);
+          Gv[k][m] = xfma(gk[b][k], vk[b][m], Gv[k][m]);
         }
       }
     }
@@ -266,9 +278,10 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          KT t = alpha * p[a][k] + beta * tc.c * q[a][k];
+          KT t = xfma(alpha, p[a][k], xmul(xmul(beta, tc.c), q[a][k]));
 #pragma unroll
-          for (int m = 0; m < 3; ++m) t += Pv[k][m] * (tc.hb * p[a][m]) + tc.phi * gk[a][m] * Gv[m][k];
+          for (int m = 0; m < 3; ++m)
+            t = xadd(t, xfma(Pv[k][m], xmul(tc.hb, p[a][m]), xmul(xmul(tc.phi, gk[a][m]), Gv[m][k])));
           yr[3 * a + k] = (double)t;
         }
     } else {
@@ -381,7 +394,7 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
       tc.c *= ct;
       tc.phi *= ct;
       const double mu_k = A.mu_e ? A.mu_e[e] : A.mu0;
-      const double lam_k = A.mu_e ? (A.kappa_e[e] - (2.0 / 3.0) * A.mu_e[e]) : A.lam0;
+      const double lam_k = A.mu_e ? dfma(-2.0 / 3.0, A.mu_e[e], A.kappa_e[e]) : A.lam0;
       e_lam = (KT)(A.c_0 * G.V * lam_k);
       e_mu = (KT)(A.c_0 * G.V * mu_k);
       e_mass = (KT)(A.c_m * A.rho * fabs(G.V) * (1.0 / 20.0));  // element/tet4_base.py:138-151
@@ -444,9 +457,9 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     for (int b = 0; b < 4; ++b)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        w[b][k] = tc.A * p[b][k] + tc.c * q[b][k];
-        h[b][k] = tc.hb * p[b][k];
-        y[b][k] = tc.c * q[b][k];
+        w[b][k] = xfma(tc.A, p[b][k], xmul(tc.c, q[b][k]));
+        h[b][k] = xmul(tc.hb, p[b][k]);
+        y[b][k] = xmul(tc.c, q[b][k]);
       }
     const int gid[4] = {cn.x, cn.y, cn.z, cn.w};
     int slot = 0;
@@ -454,16 +467,18 @@ __device__ __forceinline__ void tet4_element(const Tet4Args& A, int64_t e, KT* _
     for (int a = 0; a < 4; ++a) {
 #pragma unroll
       for (int b = a; b < 4; ++b) {
-        const KT gg = gk[a][0] * gk[b][0] + gk[a][1] * gk[b][1] + gk[a][2] * gk[b][2];
-        KT s = tc.phi * gg;
-        if constexpr (kEff) s += e_mu * gg + e_mass * (a == b ? (KT)2 : (KT)1);
+        const KT gg = xdot3(gk[a][0], gk[b][0], gk[a][1], gk[b][1], gk[a][2], gk[b][2]);
+        KT s = xmul(tc.phi, gg);
+        if constexpr (kEff) s = xadd(s, xfma(e_mu, gg, xmul(e_mass, a == b ? (KT)2 : (KT)1)));
         KT v[9];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
           for (int m = 0; m < 3; ++m) {
-            v[3 * k + m] = p[a][k] * w[b][m] + p[b][k] * h[a][m] + y[a][k] * p[b][m] + (k == m ? s : (KT)0);
-            if constexpr (kEff) v[3 * k + m] += e_lam * gk[a][k] * gk[b][m] + e_mu * gk[b][k] * gk[a][m];
+            const KT last = k == m ? xfma(y[a][k], p[b][m], s) : xmul(y[a][k], p[b][m]);
+            v[3 * k + m] = xfma(p[a][k], w[b][m], xfma(p[b][k], h[a][m], last));
+            if constexpr (kEff)
+              v[3 * k + m] = xadd(v[3 * k + m], xfma(xmul(e_lam, gk[a][k]), gk[b][m], xmul(xmul(e_mu, gk[b][k]), gk[a][m])));
           }
         if (b == a) {
           const KT d[6] = {v[0], v[1], v[2], v[4], v[5], v[8]};
@@ -515,11 +530,15 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Start copying tile t's meta block into the warp's list area.
+// Start copying tile t's meta block into the warp's list area: the whole block for a
+// sweep with a tangent, the count bytes and node lists (its first meta_node_bytes) for
+// the sweeps without one (f-only 20.5 -> 8.5 bytes of lists per element).
+template <bool WANT_K>
 __device__ __forceinline__ void tile_meta_prefetch(const GatherArgs& g, int64_t t, unsigned char* lst) {
   const int lane = threadIdx.x & 31;
   const uint4* src = reinterpret_cast<const uint4*>(g.tile_meta + t * g.meta_stride);
-  for (int c = lane; c < g.meta_stride / 16; c += 32) cp_async16(lst + 16 * c, src + c);
+  const int chunks = (WANT_K ? g.meta_stride : g.meta_node_bytes) / 16;
+  for (int c = lane; c < chunks; c += 32) cp_async16(lst + 16 * c, src + c);
 }
 
 // Sum the staged element blocks of tile `t` into its tile record (one warp), with the
@@ -625,11 +644,11 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
       // a tile is `g.tile` consecutive elements starting at a multiple of g.tile; its
       // lists arrive in shared memory while the elements are evaluated
       const int64_t t = task.z / g.tile;
-      tile_meta_prefetch(g, t, lst);
+      tile_meta_prefetch<S::kWantK>(g, t, lst);
       const int64_t e = task.z + (int64_t)lane;
       if (e < task.w)
-        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
-                                             fst + kFStride * lane);
+        tet4_element<KT, MODE, false, false>(A, e, __ldg(reinterpret_cast<const int4*>(A.conn) + e),
+                                             reinterpret_cast<KT*>(kst + lane * kStageStride), fst + kFStride * lane);
       cp_async_wait_all();
       __syncwarp();
       tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
@@ -637,7 +656,8 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
     } else {
       for (int64_t e = task.z + (int64_t)lane; e < task.w; e += 32) {
         const int64_t slot = e & g.ring_mask;
-        tet4_element<KT, MODE>(A, e, krec + slot * (16 / (int64_t)sizeof(KT)), frec + slot * 2);  // planar records
+        tet4_element<KT, MODE>(A, e, __ldg(reinterpret_cast<const int4*>(A.conn) + e),
+                               krec + slot * (16 / (int64_t)sizeof(KT)), frec + slot * 2);  // planar records
       }
     }
   };
@@ -670,8 +690,10 @@ tet4_persistent_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, KT* __restrict__ k
 #ifndef PSX_SPLIT_NODE_BATCH
 #define PSX_SPLIT_NODE_BATCH 1
 #endif
+// 160 element / 96 gather registers: the gathers hold the next task's item heads, which
+// spill at 80 registers
 #ifndef PSX_SPLIT_ELEM_REGS
-#define PSX_SPLIT_ELEM_REGS 176
+#define PSX_SPLIT_ELEM_REGS 160
 #endif
 #ifndef PSX_SPLIT_ELEM_WARPS
 #define PSX_SPLIT_ELEM_WARPS 8
@@ -711,15 +733,17 @@ tet4_split_kernel(Tet4Args A, GatherArgs g, QueueArgs Q, const int4* __restrict_
     float* kst = reinterpret_cast<float*>(my_stage);
     double* fst = reinterpret_cast<double*>(my_stage + sizeof(float) * S::kKFloats);
     unsigned char* lst = my_stage + sizeof(float) * S::kKFloats + sizeof(double) * S::kFDoubles;
-    drain_elements(Q, ecnt, A.st, [&](const int4& task) {
+    drain_elements(Q, reinterpret_cast<const int4*>(A.conn), ecnt, A.st,
+                   [&](const int4& task, const int4 cn, auto&& publish_previous) {
       const int64_t t = task.z / g.tile;
-      tile_meta_prefetch(g, t, lst);
+      tile_meta_prefetch<S::kWantK>(g, t, lst);
       const int64_t e = task.z + (int64_t)lane;
       if (e < task.w)
-        tet4_element<KT, MODE, false, false>(A, e, reinterpret_cast<KT*>(kst + lane * kStageStride),
+        tet4_element<KT, MODE, false, false>(A, e, cn, reinterpret_cast<KT*>(kst + lane * kStageStride),
                                              fst + kFStride * lane);
       cp_async_wait_all();
       __syncwarp();
+      publish_previous();
       tile_reduce<S::kWantK, S::kWantF>(g, t, lst, kst, fst, reinterpret_cast<float*>(krec), frec);
       __syncwarp();
     });

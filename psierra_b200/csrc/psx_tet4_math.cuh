@@ -31,7 +31,7 @@ __device__ __forceinline__ void tet4_geometry(const double Xn[4][3], Tet4Geom& G
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) D[i][j] = Xn[j + 1][i] - Xn[0][i];
+    for (int j = 0; j < 3; ++j) D[i][j] = dsub(Xn[j + 1][i], Xn[0][i]);
   G.detD = inv3(D, Di);
   G.V = G.detD / 6.0;
 #pragma unroll
@@ -39,7 +39,7 @@ __device__ __forceinline__ void tet4_geometry(const double Xn[4][3], Tet4Geom& G
     G.g[1][j] = Di[0][j];
     G.g[2][j] = Di[1][j];
     G.g[3][j] = Di[2][j];
-    G.g[0][j] = -(Di[0][j] + Di[1][j] + Di[2][j]);
+    G.g[0][j] = -dadd(dadd(Di[0][j], Di[1][j]), Di[2][j]);
   }
 }
 
@@ -49,10 +49,8 @@ __device__ __forceinline__ void tet4_grad(const double Un[4][3], const Tet4Geom&
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      double v = 0.0;
-#pragma unroll
-      for (int b = 1; b < 4; ++b) v += (Un[b][i] - Un[0][i]) * G.g[b][j];
-      l[i][j] = v;
+      l[i][j] = ddot3(dsub(Un[1][i], Un[0][i]), G.g[1][j], dsub(Un[2][i], Un[0][i]), G.g[2][j],
+                      dsub(Un[3][i], Un[0][i]), G.g[3][j]);
     }
 }
 

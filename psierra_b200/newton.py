@@ -31,6 +31,7 @@ class DeviceNewtonResult:
     iteration_history: list[int] = field(default_factory=list)
     pcg_iterations: list[int] = field(default_factory=list)
     residual_history: list[float] = field(default_factory=list)
+    step_lengths: list[float] = field(default_factory=list)  # accepted line-search alphas
 
 
 class DeviceNewton:
@@ -90,7 +91,7 @@ class DeviceNewton:
         n = self.n
         u = torch.zeros(n, dtype=torch.float64, device=self.asm.device) if u0 is None else u0.clone()
         up = torch.zeros_like(u) if u_prescribed is None else u_prescribed
-        hist, pcg_its, rhist = [], [], []
+        hist, pcg_its, rhist, alphas = [], [], [], []
         for step in range(1, n_steps + 1):
             lam = step / n_steps
             u_acc = u.clone()
@@ -129,11 +130,12 @@ class DeviceNewton:
                 if not res.success:
                     break
                 u = u + res.alpha * du
+                alphas.append(float(res.alpha))
             if not converged:
-                return DeviceNewtonResult(u_acc, False, step - 1, hist, pcg_its, rhist)
+                return DeviceNewtonResult(u_acc, False, step - 1, hist, pcg_its, rhist, alphas)
             hist.append(it)
         u = self._polish(u, f_step, rhist[-1], polish, pcg_its, rhist)
-        return DeviceNewtonResult(u, True, n_steps, hist, pcg_its, rhist)
+        return DeviceNewtonResult(u, True, n_steps, hist, pcg_its, rhist, alphas)
 
     def _polish(self, u, f_step, rn, n_extra, pcg_its, rhist):
         for _ in range(n_extra):

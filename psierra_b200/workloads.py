@@ -40,7 +40,8 @@ def _nh(E, nu, rho=1000.0):
     return NeoHookean(p)
 
 
-def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), pcg_rtol: float = 1e-8) -> dict:
+def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), pcg_rtol: float = 1e-8,
+         nr_iterations: int = 30) -> dict:
     m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, cells, cells, cells))
     bottom = meshgen.nodes_on_plane(m, 2, "min")
     top = meshgen.nodes_on_plane(m, 2, "max")
@@ -50,14 +51,15 @@ def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), 
     up[torch.from_numpy(3 * top + 2).to(dev)] = -0.2
     f_ext = torch.zeros(m.n_dofs, dtype=torch.float64, device=dev)
     out = {"workload": f"cfg3: cube {cells}^3 Kuhn -> {m.n_elements} Tet10, {m.n_nodes} nodes ({m.n_dofs} DOFs), "
-                       f"E=1e4 nu=0.4, top u_z=-0.2 over {n_steps} increments, Jacobi PCG rtol {pcg_rtol}"}
+                       f"E=1e4 nu=0.4, top u_z=-0.2 over {n_steps} increments, Jacobi PCG rtol {pcg_rtol}, "
+                       f"at most {nr_iterations} Newton iterations per increment"}
     us = {}
     for prec in precisions:
         asm = GPUAssembler(m.nodes, m.elements, _nh(1e4, 0.4), precision=prec)
         nt = DeviceNewton(asm, fixed, precision=prec, pcg_tol=pcg_rtol, pcg_maxiter=100000, preconditioner="jacobi")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = nt.solve(f_ext, u_prescribed=up, n_steps=n_steps, nr_iterations=30, nr_tol=1e-8)
+        res = nt.solve(f_ext, u_prescribed=up, n_steps=n_steps, nr_iterations=nr_iterations, nr_tol=1e-8)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         us[prec] = res.u
@@ -68,7 +70,8 @@ def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), 
             "final_relative_residual": (res.residual_history[-1] / max(res.residual_history[0], 1e-300)
                                         if res.residual_history else None),
             "first_residuals": [float(r) for r in res.residual_history[:32]],
-            "first_pcg_iterations": [int(i) for i in res.pcg_iterations[:32]]}
+            "first_pcg_iterations": [int(i) for i in res.pcg_iterations[:32]],
+            "first_step_lengths": [round(a, 6) for a in res.step_lengths[:32]]}
     if "fp64" in us and "fp32-mixed" in us:
         out["u_mixed_vs_fp64_rel2"] = float((us["fp32-mixed"] - us["fp64"]).norm() / us["fp64"].norm())
     return out
@@ -136,7 +139,11 @@ def cfg4(h_grid: float = 0.002, gravity_fraction: float = 0.2, n_check: int = 32
             "forward_plus_adjoint_seconds": t_grad, "fd_seconds": t_fd, "fd_elements": int(n_check),
             "fd_relative_step": rel_step, "max_rel_error": float(max(errs)), "median_rel_error": float(np.median(errs)),
             "rel_errors": [float(x) for x in errs],
-            "relative_sensitivity": [float(abs(fd) * mu0[e] / Lv) for fd, e in zip(fds, picks)]}
+            "relative_sensitivity": [float(abs(fd) * mu0[e] / Lv) for fd, e in zip(fds, picks)],
+            # |adjoint - central difference| in units of L / mu_e: a constant floor here means
+            # the difference quotient's rounding (the forward solve's error in L over 2h), not
+            # the adjoint, sets the relative errors of the least sensitive elements
+            "abs_error_rel_units": [float(abs(g[e] - fd) * mu0[e] / Lv) for fd, e in zip(fds, picks)]}
 
 
 def cfg5(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, pcg_iterations: int = 16000,
@@ -170,6 +177,10 @@ def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("workload", choices=["cfg3", "cfg4", "cfg5"])
     ap.add_argument("--cells", type=int, default=30, help="cfg3: cube cells per side")
+    ap.add_argument("--steps", type=int, default=20, help="cfg3: increments")
+    ap.add_argument("--nr-iterations", type=int, default=30, help="cfg3: Newton iterations per increment")
+    ap.add_argument("--pcg-rtol", type=float, default=1e-8, help="cfg3: PCG relative tolerance")
+    ap.add_argument("--precisions", default="fp64,fp32-mixed", help="cfg3: comma-separated precisions")
     ap.add_argument("--grid", type=float, default=0.002, help="cfg4: grid spacing (m)")
     ap.add_argument("--gravity", type=float, default=0.2, help="cfg4: fraction of gravity")
     ap.add_argument("--fd-elements", type=int, default=32, help="cfg4: elements checked by central differences")
@@ -177,7 +188,8 @@ def main(argv=None) -> None:
     ap.add_argument("--beams", type=int, default=256, help="cfg5: instances")
     a = ap.parse_args(argv)
     if a.workload == "cfg3":
-        rec = cfg3(cells=a.cells)
+        rec = cfg3(cells=a.cells, n_steps=a.steps, precisions=tuple(a.precisions.split(",")), pcg_rtol=a.pcg_rtol,
+                   nr_iterations=a.nr_iterations)
     elif a.workload == "cfg4":
         rec = cfg4(h_grid=a.grid, gravity_fraction=a.gravity, n_check=a.fd_elements, rel_step=a.fd_step)
     else:

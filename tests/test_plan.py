@@ -101,10 +101,10 @@ def tile_meta(h, T, t):
     """(np, nn, pair offsets, node offsets, pair codes, node codes) of tile t."""
     m = h["tile_meta"][t * h["tile_meta_stride"]:(t + 1) * h["tile_meta_stride"]].astype(np.int64)
     up4 = lambda b: (b + 3) // 4 * 4  # noqa: E731
-    off_p = 4
-    off_n = off_p + up4(6 * T + 1)
-    src_p = off_n + up4(4 * T + 1)
-    src_n = src_p + 6 * T
+    off_n = 4
+    src_n = off_n + up4(4 * T + 1)
+    off_p = src_n + 4 * T
+    src_p = off_p + up4(6 * T + 1)
     n_p, n_n = int(m[0]), int(m[1])
     return (n_p, n_n, m[off_p:off_p + n_p + 1], m[off_n:off_n + n_n + 1], m[src_p:src_p + 6 * T],
             m[src_n:src_n + 4 * T])

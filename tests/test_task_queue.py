@@ -3,9 +3,12 @@
 The kernel's wait rules, restated:
 * gather tiles of granule r are queued after the element tiles of granule r + 1 + lag;
 * an element tile of granule g waits for all gather tiles of granules
-  [g - R, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
+  [0, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
   slots of granule g - R, if g - R >= 0;
-* a gather tile of granule r waits for all element tiles of granules [r - span_g - 1, r].
+* a gather tile of granule r waits for all element tiles of granules [0, r].
+Both waits are on prefixes (each warp keeps a watermark of the granules it knows are
+complete); the spans the ring needs, [g - R, g - R + span_g + 1] and [r - span_g - 1, r],
+are inside them.
 Tasks are claimed in queue order by running blocks, so the queue always drains if every
 task only waits on tasks strictly earlier in the queue.  Ring safety: every gather item
 that reads an element of granule q belongs to a granule in [q, q + span_g + 1].
@@ -74,10 +77,10 @@ def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
         if kind == 0:
             old = g - ring
             if old >= 0:
-                for r in range(old, min(old + span_g + 2, G)):
+                for r in range(0, min(old + span_g + 2, G)):
                     assert last_b.get(r, -1) < q, "element tile waits on a later gather tile"
         else:
-            for gp in range(max(0, g - span_g - 1), g + 1):
+            for gp in range(0, g + 1):
                 assert last_a[gp] < q, "gather tile waits on a later element tile"
     # ring safety: items read elements within span_g + 1 granules of their own granule
     for kind, g, b, e in tasks[kinds != 0]:
@@ -118,9 +121,9 @@ def test_split_queues_drain(granule, lag, workers, seed):
     def ready(role, t):
         if role == "e":
             old = t * tile // granule - ring
-            return old < 0 or all(done_b[r] >= bt[r] for r in range(old, min(old + span_g + 2, G)))
+            return old < 0 or all(done_b[r] >= bt[r] for r in range(0, min(old + span_g + 2, G)))
         g = gtasks[t, 1]
-        return all(done_a[r] >= atiles[r] for r in range(max(0, g - span_g - 1), g + 1))
+        return all(done_a[r] >= atiles[r] for r in range(0, g + 1))
 
     remaining = n_tiles + len(gtasks)
     while remaining:
@@ -174,3 +177,91 @@ def test_split_plan_lists_the_gather_tasks_in_queue_order():
     p.set_queue(lag=3)
     d2 = p.device("cpu")
     assert np.array_equal(d2["gtasks_k"].numpy().reshape(-1, 4), gk)
+
+
+@pytest.mark.parametrize("granule,lag,workers,seed", [(128, 0, (1, 1), 4), (128, 2, (3, 2), 5), (64, 0, (4, 4), 6),
+                                                      (64, 1, (2, 1), 7)])
+def test_split_queues_drain_with_deferred_publish(granule, lag, workers, seed):
+    """Element warps claim tiles two ahead (they hold the tile they work on and the next
+    one) and publish a finished tile only once their next tile has been evaluated, or
+    earlier when that next tile's ring wait is not yet satisfied (psx_gather.cuh
+    drain_elements).  Waits are on prefixes.  A random schedule must still drain."""
+    m = meshgen.box_tet4(1.0, 1.0, 1.0, 9, 8, 7)
+    p = MeshPattern(m.elements, m.n_nodes)
+    p.granule = granule
+    tile = 32
+    tasks, bt, h = _queue(p, 1, tile, lag)
+    G = h["n_granules"]
+    span_g = -(-int(h["max_span"][0]) // granule)
+    all_g = 1 << int(np.ceil(np.log2(max(G, 1))))
+    ring = min(1 << int(np.ceil(np.log2(span_g + lag + 6))), all_g)
+    n_tiles = -(-m.n_elements // tile)
+    gtasks = tasks[tasks[:, 0] != 0]
+    atiles = [-(-min(granule, m.n_elements - r * granule) // tile) for r in range(G)]
+    done_a = np.zeros(G, dtype=np.int64)
+    done_b = np.zeros(G, dtype=np.int64)
+    rng = np.random.default_rng(seed)
+    nxt = {"e": 0, "g": 0}
+    # element worker: [claimed tiles (at most two, the first is worked on), evaluated?,
+    # pending (finished, unpublished) tile or None]
+    ew = [[[], False, None] for _ in range(workers[0])]
+    gw = [None] * workers[1]
+
+    def e_ready(t):
+        old = t * tile // granule - ring
+        return old < 0 or all(done_b[r] >= bt[r] for r in range(0, min(old + span_g + 2, G)))
+
+    def g_ready(t):
+        return all(done_a[r] >= atiles[r] for r in range(0, gtasks[t, 1] + 1))
+
+    def publish(w):
+        if w[2] is not None:
+            done_a[w[2] * tile // granule] += 1
+            w[2] = None
+
+    remaining = n_tiles + len(gtasks)
+    while remaining or any(w[2] is not None for w in ew):
+        moves = []
+        for i, w in enumerate(ew):
+            if len(w[0]) < 2 and nxt["e"] < n_tiles:
+                moves.append(("claim_e", i))
+            if not w[0]:
+                if nxt["e"] >= n_tiles and w[2] is not None:
+                    moves.append(("flush", i))  # the queue is empty: publish and leave
+            elif not w[1]:
+                if e_ready(w[0][0]):
+                    moves.append(("eval", i))
+                elif w[2] is not None:
+                    moves.append(("flush", i))  # about to block: publish first
+            else:
+                moves.append(("finish", i))
+        for i, t in enumerate(gw):
+            if t is None:
+                if nxt["g"] < len(gtasks):
+                    moves.append(("claim_g", i))
+            elif g_ready(t):
+                moves.append(("gather", i))
+        assert moves, "split queues deadlocked"
+        kind, i = moves[rng.integers(len(moves))]
+        if kind == "claim_e":
+            ew[i][0].append(nxt["e"])
+            nxt["e"] += 1
+        elif kind == "flush":
+            publish(ew[i])
+        elif kind == "eval":
+            ew[i][1] = True
+            publish(ew[i])  # the previous tile goes out after this tile's evaluation
+        elif kind == "finish":
+            ew[i][2], ew[i][1] = ew[i][0].pop(0), False
+            remaining -= 1
+        elif kind == "claim_g":
+            gw[i] = nxt["g"]
+            nxt["g"] += 1
+        else:
+            t = gw[i]
+            g = gtasks[t, 1]
+            assert all(done_a[r] >= atiles[r] for r in range(max(0, g - span_g - 1), g + 1))
+            done_b[g] += 1
+            gw[i] = None
+            remaining -= 1
+    assert (done_a == np.array(atiles)).all() and (done_b == bt).all()
