@@ -419,6 +419,51 @@ int psx_pcg_enqueue(int64_t n, const int32_t* indptr, const int32_t* indices, co
                     int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
                     int precond, void* work, int64_t work_bytes, void* status, void* stream);
 
+/* ---- Two-level preconditioner (no counterpart in the reference) -------------------
+ * A coarse space of rigid-body modes: the nodes are grouped into aggregates, and each
+ * aggregate a contributes six columns of the prolongation P (three translations and
+ * three rotations about its centroid: the column of rotation e at node i is
+ * e x (X_i - c_a)); P is zero on eliminated unknowns.  The preconditioner is
+ *   M^-1 r = B^-1 r + P A_c^-1 P^T r,    A_c = P^T A P,
+ * with B the 3x3 diagonal blocks of A (block-Jacobi).  The aggregates are grouped into
+ * independent blocks (the instances of a batch of meshes, whose A is block diagonal), and
+ * the caller supplies A_c^-1 of every block as a dense matrix (psx_coarse_probe and
+ * psx_coarse_restrict assemble A_c from products with A). */
+typedef struct psx_coarse_t {
+  int64_t n_nodes;           /* N: the system has 3N unknowns */
+  int64_t n_agg;             /* aggregates */
+  const int32_t* node_agg;   /* N: aggregate of each node, or -1 */
+  const int32_t* agg_ptr;    /* n_agg + 1: nodes of aggregate a are agg_nodes[agg_ptr[a] .. agg_ptr[a+1]) */
+  const int32_t* agg_nodes;  /* ascending within each aggregate */
+  const double* d;           /* N x 3: node coordinates minus the centroid of its aggregate */
+  const uint8_t* fixed;      /* 3N: nonzero on eliminated unknowns */
+  int32_t n_blocks;          /* independent coarse blocks */
+  int32_t nc;                /* padded coarse size: >= 6 x the aggregates of any block */
+  const int32_t* block_agg;  /* n_blocks + 1: block b holds aggregates [block_agg[b], block_agg[b+1]) */
+  const double* ainv;        /* n_blocks x nc x nc, row-major: A_c^-1 of each block (6 (a - block_agg[b]) + t) */
+  double* rc;                /* 6 n_agg scratch */
+  double* yc;                /* 6 n_agg scratch */
+} psx_coarse_t;
+
+/* v (3N, device) = sum over the aggregates a with agg_color[a] == color of column
+ * 6 a + mode of P (mode 0-2 translations, 3-5 rotations). */
+int psx_coarse_probe(const psx_coarse_t* coarse, const int32_t* agg_color, int32_t color, int32_t mode, double* v,
+                     void* stream);
+
+/* out (6 n_agg, device) = P^T w, each aggregate's six sums in a fixed order. */
+int psx_coarse_restrict(const psx_coarse_t* coarse, const double* w, double* out, void* stream);
+
+/*
+ * psx_pcg / psx_pcg_enqueue with the two-level preconditioner: precond must be
+ * PSX_PRECOND_BJACOBI (optionally | PSX_PCG_NODAL); the coarse correction is added to
+ * every block-Jacobi application.  host_checks = 1 behaves as psx_pcg (a stream
+ * synchronisation every 16 iterations), 0 as psx_pcg_enqueue (capturable).
+ */
+int psx_pcg_coarse(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                   int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+                   int precond, const psx_coarse_t* coarse, void* work, int64_t work_bytes, void* status,
+                   void* stream, int host_checks);
+
 /*
  * y = alpha A x + beta y for a CSR matrix (values double for PSX_FP64, float for
  * PSX_FP32_MIXED; x, y double, device), rows summed in a fixed order: the products with

@@ -81,6 +81,9 @@ SIGNATURES: dict[str, list] = {
     "psx_tet4_split_ready": [],
     "psx_fma_roof": [_i32, _i64, _i32, _p, _p, _p],
     "psx_fma_roof_sink_bytes": [_i32],
+    "psx_coarse_probe": [_p, _p, _i32, _i32, _p, _p],
+    "psx_coarse_restrict": [_p, _p, _p, _p],
+    "psx_pcg_coarse": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _p, _i64, _p, _p, _i32],
 }
 
 
@@ -128,6 +131,26 @@ class PlanStruct(ctypes.Structure):
         ("gtasks_k", ctypes.c_void_p),
         ("wait_spins", ctypes.c_int32),
         ("reserved0", ctypes.c_int32),
+    ]
+
+
+class CoarseStruct(ctypes.Structure):
+    """Mirror of ``psx_coarse_t`` (include/psierra_b200.h)."""
+
+    _fields_ = [
+        ("n_nodes", ctypes.c_int64),
+        ("n_agg", ctypes.c_int64),
+        ("node_agg", ctypes.c_void_p),
+        ("agg_ptr", ctypes.c_void_p),
+        ("agg_nodes", ctypes.c_void_p),
+        ("d", ctypes.c_void_p),
+        ("fixed", ctypes.c_void_p),
+        ("n_blocks", ctypes.c_int32),
+        ("nc", ctypes.c_int32),
+        ("block_agg", ctypes.c_void_p),
+        ("ainv", ctypes.c_void_p),
+        ("rc", ctypes.c_void_p),
+        ("yc", ctypes.c_void_p),
     ]
 
 

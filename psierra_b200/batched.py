@@ -13,7 +13,9 @@ iteration for the whole batch is one replay of a captured CUDA graph:
   fused f_int + K_T assembly -> symmetric elimination of the clamped DOFs ->
   R = lambda f_ext - f_int on the free DOFs -> per-instance ||R|| (fixed-order segment
   sums) -> instance mask (||R_i|| >= tol_i) -> rhs R_i / ref_i on active instances ->
-  PCG with a fixed trip count (block-Jacobi) -> du_i = ref_i * solution -> u += du.
+  PCG with a fixed trip count (block-Jacobi, or block-Jacobi with the rigid-body-mode
+  coarse correction of ``psierra_b200.coarse``, whose coarse matrices are refreshed from
+  the new tangent inside the same replay) -> du_i = ref_i * solution -> u += du.
 
 The system is block diagonal, so scaling instance i's right-hand side by 1/ref_i
 (ref_i = ||lambda f_ext,i||) scales only that instance's solution: every instance gets
@@ -120,8 +122,11 @@ class BatchedNewtonResult:
 
 class BatchedNewton:
     def __init__(self, batch: MeshBatch, fixed_dofs, precision: str | None = None, pcg_iterations: int = 500,
-                 pcg_rtol: float = 1e-8, preconditioner: str = "block-jacobi", use_graph: bool = True):
-        """``fixed_dofs``: per instance, its clamped DOFs in local numbering."""
+                 pcg_rtol: float = 1e-8, preconditioner: str = "block-jacobi", use_graph: bool = True,
+                 nodes_per_aggregate: int = 500):
+        """``fixed_dofs``: per instance, its clamped DOFs in local numbering.
+        ``preconditioner``: "none", "jacobi", "block-jacobi" or "two-level" (block-Jacobi
+        plus rigid-body modes of slices of about ``nodes_per_aggregate`` nodes)."""
         self.batch = batch
         asm = batch.asm
         self.asm = asm
@@ -140,7 +145,14 @@ class BatchedNewton:
         self.pcg_rtol = float(pcg_rtol)
         # the batch's CSR has the assembler's node-blocked layout (PSX_PCG_NODAL)
         self.precond = {"none": _lib.PSX_PRECOND_NONE, "jacobi": _lib.PSX_PRECOND_JACOBI,
-                        "block-jacobi": _lib.PSX_PRECOND_BJACOBI}[preconditioner] | _lib.PSX_PCG_NODAL
+                        "block-jacobi": _lib.PSX_PRECOND_BJACOBI,
+                        "two-level": _lib.PSX_PRECOND_BJACOBI}[preconditioner] | _lib.PSX_PCG_NODAL
+        self.coarse = None
+        if preconditioner == "two-level":
+            from psierra_b200.coarse import CoarseSpace
+
+            self.coarse = CoarseSpace(batch.mesh.nodes, batch.mesh.elements, mask, batch.node_offsets,
+                                      nodes_per_aggregate, device=dev)
         self.use_graph = use_graph
         f64 = dict(dtype=torch.float64, device=dev)
         B = batch.B
@@ -181,10 +193,17 @@ class BatchedNewton:
         torch.mul(self.r, self.inv_scale, out=self.rhs)
         self.rhs.mul_(self.act_dof)
         self.du.zero_()
-        check(lib().psx_pcg_enqueue(self.n, ptr(d["indptr"]), ptr(d["indices"]), ptr(self.k), vp, ptr(self.rhs),
-                                    ptr(self.du), self.pcg_rtol, 0.0, self.pcg_iterations, self.precond,
-                                    ptr(self.pcg_work), self.pcg_work.numel(), ptr(self.pcg_status), _stream()),
-              "psx_pcg_enqueue")
+        if self.coarse is not None:
+            self.coarse.update(self.k, d["indptr"], d["indices"])
+            check(lib().psx_pcg_coarse(self.n, ptr(d["indptr"]), ptr(d["indices"]), ptr(self.k), vp, ptr(self.rhs),
+                                       ptr(self.du), self.pcg_rtol, 0.0, self.pcg_iterations, self.precond,
+                                       self.coarse.struct_ptr(), ptr(self.pcg_work), self.pcg_work.numel(),
+                                       ptr(self.pcg_status), _stream(), 0), "psx_pcg_coarse")
+        else:
+            check(lib().psx_pcg_enqueue(self.n, ptr(d["indptr"]), ptr(d["indices"]), ptr(self.k), vp, ptr(self.rhs),
+                                        ptr(self.du), self.pcg_rtol, 0.0, self.pcg_iterations, self.precond,
+                                        ptr(self.pcg_work), self.pcg_work.numel(), ptr(self.pcg_status), _stream()),
+                  "psx_pcg_enqueue")
         self.du.mul_(self.scale)
         self.u.add_(self.du)
 

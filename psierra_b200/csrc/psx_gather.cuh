@@ -513,12 +513,15 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
 // loops cannot deadlock while the warps that claimed tasks are resident; a wait that
 // gives up flags the status and the task proceeds in bounds.
 // Tuning switches of the warp-specialised loops: load the next element tile's
-// connectivity / the next gather task's item heads while the current one runs.
+// connectivity / the next gather task's item heads while the current one runs.  On the
+// 80^3 cube (f+K) the connectivity prefetch is neutral (0.616-0.619 against
+// 0.616-0.621 ms); the head prefetch spills at 80 gather registers and, with the
+// 160 / 96 split it needs, ran 0.643 ms.
 #ifndef PSX_SPLIT_PREFETCH_CONN
 #define PSX_SPLIT_PREFETCH_CONN 1
 #endif
 #ifndef PSX_SPLIT_PREFETCH_HEADS
-#define PSX_SPLIT_PREFETCH_HEADS 1
+#define PSX_SPLIT_PREFETCH_HEADS 0
 #endif
 
 template <typename ElementTile>

@@ -369,6 +369,149 @@ __global__ void __launch_bounds__(kBlock) pcg_update_xr(int64_t n, double* __res
   }
 }
 
+// ---- two-level preconditioner: rigid-body modes per aggregate --------------------------
+// P^T w for aggregate a: translations sum w_i, rotations sum d_i x w_i (the column of
+// rotation e at node i is e x d_i, and (e x d).w = e.(d x w)).  One warp per aggregate,
+// lane sums in a fixed order.
+__global__ void __launch_bounds__(kBlock) coarse_restrict_kernel(psx_coarse_t c, const double* __restrict__ w,
+                                                                 double* __restrict__ out, const PcgScalars* s) {
+  if (s && stopped(s)) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (kBlock / 32);
+  for (int64_t a = blockIdx.x * (int64_t)(kBlock / 32) + (threadIdx.x >> 5); a < c.n_agg; a += warps) {
+    double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int32_t k = c.agg_ptr[a] + lane; k < c.agg_ptr[a + 1]; k += 32) {
+      const int64_t i = c.agg_nodes[k];
+      double v[3];
+#pragma unroll
+      for (int m = 0; m < 3; ++m) v[m] = c.fixed[3 * i + m] ? 0.0 : w[3 * i + m];
+      const double dx = c.d[3 * i], dy = c.d[3 * i + 1], dz = c.d[3 * i + 2];
+      t[0] += v[0];
+      t[1] += v[1];
+      t[2] += v[2];
+      t[3] += dy * v[2] - dz * v[1];
+      t[4] += dz * v[0] - dx * v[2];
+      t[5] += dx * v[1] - dy * v[0];
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) t[m] = warp_sum(t[m]);
+    if (lane == 0)
+#pragma unroll
+      for (int m = 0; m < 6; ++m) out[6 * a + m] = t[m];
+  }
+}
+
+// yc = A_c^-1 rc per block (one thread block each, a warp per row, lane sums in a fixed
+// order); the block's right-hand side is staged in shared memory.
+__global__ void __launch_bounds__(kBlock) coarse_gemv_kernel(psx_coarse_t c, const PcgScalars* s) {
+  if (s && stopped(s)) return;
+  extern __shared__ double s_rhs[];
+  const int32_t a0 = c.block_agg[blockIdx.x];
+  const int m = 6 * (c.block_agg[blockIdx.x + 1] - a0);
+  for (int k = threadIdx.x; k < m; k += kBlock) s_rhs[k] = c.rc[6 * (int64_t)a0 + k];
+  __syncthreads();
+  const double* A = c.ainv + (int64_t)blockIdx.x * c.nc * c.nc;
+  const int lane = threadIdx.x & 31;
+  for (int r = threadIdx.x >> 5; r < m; r += kBlock / 32) {
+    double acc = 0.0;
+    for (int k = lane; k < m; k += 32) acc += A[(int64_t)r * c.nc + k] * s_rhs[k];
+    acc = warp_sum(acc);
+    if (lane == 0) c.yc[6 * (int64_t)a0 + r] = acc;
+  }
+}
+
+// v = sum of column `mode` of P over the aggregates of colour `color`.
+__global__ void coarse_probe_kernel(psx_coarse_t c, const int32_t* __restrict__ color_of, int32_t color, int32_t mode,
+                                    double* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < c.n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = c.node_agg[i];
+    double col[3] = {0.0, 0.0, 0.0};
+    if (a >= 0 && color_of[a] == color) {
+      const double dx = c.d[3 * i], dy = c.d[3 * i + 1], dz = c.d[3 * i + 2];
+      if (mode < 3) {
+        col[mode] = 1.0;
+      } else if (mode == 3) {  // e_x x d
+        col[1] = -dz;
+        col[2] = dy;
+      } else if (mode == 4) {  // e_y x d
+        col[0] = dz;
+        col[2] = -dx;
+      } else {  // e_z x d
+        col[0] = -dy;
+        col[1] = dx;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) v[3 * i + k] = c.fixed[3 * i + k] ? 0.0 : col[k];
+  }
+}
+
+// x += alpha p; r -= alpha q (the two-level iteration forms z after the coarse solve)
+__global__ void __launch_bounds__(kBlock) pcg_update_xr_only(int64_t n, double* __restrict__ x, PcgWork w) {
+  if (stopped(w.s)) return;
+  const double alpha = w.s->alpha;
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+    x[i] += alpha * w.p[i];
+    w.r[i] -= alpha * w.q[i];
+  }
+}
+
+// z = B^-1 r + P yc per node, with r.r and r.z (and b.b on the first call) and the
+// bookkeeping of pcg_init_dots (INIT) or pcg_update_xr.
+template <bool INIT>
+__global__ void __launch_bounds__(kBlock) pcg_coarse_z(int64_t n, const double* __restrict__ b, PcgWork w,
+                                                       psx_coarse_t c, double rtol, double atol, int32_t maxiter) {
+  if (!INIT && stopped(w.s)) return;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n / 3; i += (int64_t)gridDim.x * kBlock) {
+    apply_prec<true>(w, i, w.z, w.r);
+    const int32_t a = c.node_agg[i];
+    if (a >= 0) {
+      const double* y = c.yc + 6 * (int64_t)a;
+      const double dx = c.d[3 * i], dy = c.d[3 * i + 1], dz = c.d[3 * i + 2];
+      const double add[3] = {y[0] + (y[4] * dz - y[5] * dy), y[1] + (y[5] * dx - y[3] * dz),
+                             y[2] + (y[3] * dy - y[4] * dx)};
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (!c.fixed[3 * i + k]) w.z[3 * i + k] += add[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int64_t d = 3 * i + k;
+      v[0] += w.r[d] * w.r[d];
+      v[1] += w.r[d] * w.z[d];
+      if constexpr (INIT) v[2] += b[d] * b[d];
+    }
+  }
+  PcgScalars* s = w.s;
+  if constexpr (INIT) {
+    double tot[3];
+    if (last_block_total<3>(v, w.partial, &s->ticket[0], tot)) {
+      s->rr = tot[0];
+      s->rho = tot[1];
+      s->bb = tot[2];
+      const double a = fmax(atol, rtol * sqrt(tot[2]));
+      s->atol2 = a * a;
+      s->iters = 0;
+      s->first = 1;
+      s->breakdown = 0;
+      s->converged = (tot[2] == 0.0 || sqrt(tot[0]) < a) ? 1 : 0;
+    }
+  } else {
+    double tot[2];
+    if (last_block_total<2>(v, w.partial, &s->ticket[2], tot)) {
+      s->rho_prev = s->rho;
+      s->rr = tot[0];
+      s->rho = tot[1];
+      s->first = 0;
+      s->iters += 1;
+      if (!isfinite(tot[0])) s->breakdown = 1;
+      else if (s->iters >= maxiter) s->breakdown = 2;
+      else if (tot[0] < s->atol2) s->converged = 1;
+    }
+  }
+}
+
 __global__ void pcg_report(const PcgScalars* s, Status* st) {
   st->iters = s->iters;
   st->flags = s->converged ? 0 : (s->breakdown == 2 ? 2 : 4);
@@ -435,6 +578,58 @@ int run_pcg(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* 
   return PSX_OK;
 }
 
+constexpr int kCoarseMaxNc = 6144;  // coarse size per block: its right-hand side fits 48 KB of shared memory
+
+// The two-level iteration: block-Jacobi plus the coarse correction, six kernels per
+// iteration (p update, SpMV + p.q, x/r update, restriction, coarse solve, z + dots).
+template <typename VT, bool NODAL>
+int run_pcg_coarse(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* vals, const double* b,
+                   double* x, double rtol, double atol, int32_t maxiter, const PcgWork& w, const psx_coarse_t& c,
+                   Status* st, cudaStream_t s, bool host_checks) {
+  const int grid_vec = (int)std::min<int64_t>(kGridMax, (n + kBlock - 1) / kBlock);
+  const int grid_nodes = (int)std::min<int64_t>(kGridMax, (n / 3 + kBlock - 1) / kBlock);
+  const int grid_row = NODAL ? (int)std::min<int64_t>(kGridMax, (n / 3 + kBlock / kNodeLanes - 1) / (kBlock / kNodeLanes))
+                             : (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
+  const int grid_agg = (int)std::min<int64_t>(kGridMax, (c.n_agg + kBlock / 32 - 1) / (kBlock / 32));
+  const size_t smem = sizeof(double) * (size_t)c.nc;
+  if (cudaMemsetAsync(w.s, 0, sizeof(PcgScalars), s) != cudaSuccess) return PSX_ERR_CUDA;
+  bjacobi_setup<<<grid_vec, kBlock, 0, s>>>(n / 3, indptr, indices, vals, sizeof(VT) == 4, w.minv, w.s);
+  pcg_init_residual<VT, true, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, b, x, w);
+  coarse_restrict_kernel<<<grid_agg, kBlock, 0, s>>>(c, w.r, c.rc, nullptr);
+  coarse_gemv_kernel<<<c.n_blocks, kBlock, smem, s>>>(c, nullptr);
+  pcg_coarse_z<true><<<grid_nodes, kBlock, 0, s>>>(n, b, w, c, rtol, atol, maxiter);
+  PSX_CUDA_CHECK_LAUNCH();
+  PcgScalars host;
+  int32_t done = 0;
+  constexpr int kBatchIters = 16;
+  while (done < maxiter) {
+    const int32_t batch = std::min<int32_t>(kBatchIters, maxiter - done);
+    for (int32_t k = 0; k < batch; ++k) {
+      pcg_update_p<true><<<grid_vec, kBlock, 0, s>>>(n, w);
+      pcg_spmv<VT, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, w);
+      pcg_update_xr_only<<<grid_vec, kBlock, 0, s>>>(n, x, w);
+      coarse_restrict_kernel<<<grid_agg, kBlock, 0, s>>>(c, w.r, c.rc, w.s);
+      coarse_gemv_kernel<<<c.n_blocks, kBlock, smem, s>>>(c, w.s);
+      pcg_coarse_z<false><<<grid_nodes, kBlock, 0, s>>>(n, b, w, c, rtol, atol, maxiter);
+    }
+    PSX_CUDA_CHECK_LAUNCH();
+    done += batch;
+    if (!host_checks) continue;
+    if (cudaMemcpyAsync(&host, w.s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return PSX_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PSX_ERR_CUDA;
+    if (host.converged || host.breakdown) break;
+  }
+  pcg_report<<<1, 1, 0, s>>>(w.s, st);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+bool coarse_ok(const psx_coarse_t* c) {
+  return c && c->n_nodes > 0 && c->n_agg > 0 && c->node_agg && c->agg_ptr && c->agg_nodes && c->d && c->fixed &&
+         c->n_blocks > 0 && c->nc > 0 && c->nc <= kCoarseMaxNc && c->block_agg && c->ainv && c->rc && c->yc;
+}
+
 }  // namespace
 }  // namespace psx
 
@@ -485,6 +680,53 @@ extern "C" int psx_pcg(int64_t n, const int32_t* indptr, const int32_t* indices,
                        int precond, void* work, int64_t work_bytes, void* status, void* stream) {
   return pcg_entry(n, indptr, indices, values, value_precision, b, x, rtol, atol, maxiter, precond, work, work_bytes,
                    status, stream, true);
+}
+
+extern "C" int psx_pcg_coarse(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                              int value_precision, const double* b, double* x, double rtol, double atol,
+                              int32_t maxiter, int precond, const psx_coarse_t* coarse, void* work,
+                              int64_t work_bytes, void* status, void* stream, int host_checks) {
+  using namespace psx;
+  if (n <= 0 || !indptr || !indices || !values || !b || !x || !work || !status || maxiter < 0) return PSX_ERR_ARG;
+  const bool nodal = (precond & PSX_PCG_NODAL) != 0;
+  if ((precond & ~PSX_PCG_NODAL) != PSX_PRECOND_BJACOBI || n % 3) return PSX_ERR_ARG;
+  if (!coarse_ok(coarse) || coarse->n_nodes * 3 != n) return coarse && coarse->nc > kCoarseMaxNc ? PSX_ERR_LIMIT : PSX_ERR_ARG;
+  if (value_precision != PSX_FP64 && value_precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  PcgWork w;
+  int64_t need = 0;
+  int rc = layout(n, PSX_PRECOND_BJACOBI, work, &w, &need);
+  if (rc != PSX_OK) return rc;
+  if (work_bytes < need) return PSX_ERR_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Status* st = static_cast<Status*>(status);
+  const bool hc = host_checks != 0;
+  if (value_precision == PSX_FP64) {
+    const double* v = static_cast<const double*>(values);
+    return nodal ? run_pcg_coarse<double, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc)
+                 : run_pcg_coarse<double, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc);
+  }
+  const float* v = static_cast<const float*>(values);
+  return nodal ? run_pcg_coarse<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc)
+               : run_pcg_coarse<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc);
+}
+
+extern "C" int psx_coarse_probe(const psx_coarse_t* coarse, const int32_t* agg_color, int32_t color, int32_t mode,
+                                double* v, void* stream) {
+  using namespace psx;
+  if (!coarse_ok(coarse) || !agg_color || !v || mode < 0 || mode > 5) return PSX_ERR_ARG;
+  const int grid = (int)std::min<int64_t>(kGridMax, (coarse->n_nodes + kBlock - 1) / kBlock);
+  coarse_probe_kernel<<<grid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(*coarse, agg_color, color, mode, v);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
+extern "C" int psx_coarse_restrict(const psx_coarse_t* coarse, const double* w, double* out, void* stream) {
+  using namespace psx;
+  if (!coarse_ok(coarse) || !w || !out) return PSX_ERR_ARG;
+  const int grid = (int)std::min<int64_t>(kGridMax, (coarse->n_agg + kBlock / 32 - 1) / (kBlock / 32));
+  coarse_restrict_kernel<<<grid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(*coarse, w, out, nullptr);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
 }
 
 extern "C" int psx_pcg_enqueue(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,

@@ -146,8 +146,8 @@ def cfg4(h_grid: float = 0.002, gravity_fraction: float = 0.2, n_check: int = 32
             "abs_error_rel_units": [float(abs(g[e] - fd) * mu0[e] / Lv) for fd, e in zip(fds, picks)]}
 
 
-def cfg5(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, pcg_iterations: int = 16000,
-         n_steps: int = 8) -> dict:
+def cfg5(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, pcg_iterations: int | None = None,
+         n_steps: int = 8, preconditioner: str = "two-level") -> dict:
     from psierra_b200.batched import BatchedNewton, MeshBatch
 
     cases = meshgen.beam_batch(n=n, target_tets=target_tets, seed=seed)
@@ -160,7 +160,13 @@ def cfg5(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, pcg_iterations
         clamp = meshgen.nodes_on_plane(c.mesh, 0, "min")
         fixed.append(np.concatenate([3 * clamp + k for k in range(3)]))
     batch = MeshBatch([c.mesh for c in cases], mus, kappas, precision="fp32-mixed")
-    solver = BatchedNewton(batch, fixed, pcg_iterations=pcg_iterations, use_graph=True)
+    if pcg_iterations is None:
+        # block-Jacobi needs O(10^4) CG iterations per Newton step on these beams (fewer
+        # stall the Newton iteration); the rigid-body-mode coarse correction a few hundred
+        pcg_iterations = 16000 if preconditioner == "block-jacobi" else 600
+    t_setup = time.perf_counter()
+    solver = BatchedNewton(batch, fixed, pcg_iterations=pcg_iterations, use_graph=True, preconditioner=preconditioner)
+    t_setup = time.perf_counter() - t_setup
     f_ext = batch.concat(forces)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -168,8 +174,9 @@ def cfg5(n: int = 256, target_tets: float = 4.1e6, seed: int = 5, pcg_iterations
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     return {"workload": f"cfg5: {n} beams, {batch.mesh.n_elements} Tet4 in total, FP32-mixed, {n_steps} increments, "
-                        f"batched Newton as one CUDA graph per iteration, block-Jacobi CG {pcg_iterations} iterations",
-            "elements": batch.mesh.n_elements, "seconds": dt, "replays": res.replays,
+                        f"batched Newton as one CUDA graph per iteration, {preconditioner} CG {pcg_iterations} iterations",
+            "elements": batch.mesh.n_elements, "seconds": dt, "solver_setup_seconds": t_setup, "replays": res.replays,
+            "newton_per_step_max": [int(x) for x in res.iterations.max(axis=1)],
             "converged": int(res.converged.sum()), "instances": n}
 
 
@@ -186,6 +193,8 @@ def main(argv=None) -> None:
     ap.add_argument("--fd-elements", type=int, default=32, help="cfg4: elements checked by central differences")
     ap.add_argument("--fd-step", type=float, default=1e-6, help="cfg4: central-difference step / mu_e")
     ap.add_argument("--beams", type=int, default=256, help="cfg5: instances")
+    ap.add_argument("--preconditioner", default="two-level", help="cfg5: block-jacobi or two-level")
+    ap.add_argument("--pcg-iterations", type=int, default=None, help="cfg5: CG iterations per Newton step")
     a = ap.parse_args(argv)
     if a.workload == "cfg3":
         rec = cfg3(cells=a.cells, n_steps=a.steps, precisions=tuple(a.precisions.split(",")), pcg_rtol=a.pcg_rtol,
@@ -193,7 +202,8 @@ def main(argv=None) -> None:
     elif a.workload == "cfg4":
         rec = cfg4(h_grid=a.grid, gravity_fraction=a.gravity, n_check=a.fd_elements, rel_step=a.fd_step)
     else:
-        rec = cfg5(n=a.beams, target_tets=4.1e6 * a.beams / 256)
+        rec = cfg5(n=a.beams, target_tets=4.1e6 * a.beams / 256, preconditioner=a.preconditioner,
+                   pcg_iterations=a.pcg_iterations)
     print(json.dumps(rec))
 
 
