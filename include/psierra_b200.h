@@ -465,6 +465,28 @@ int psx_pcg_coarse(int64_t n, const int32_t* indptr, const int32_t* indices, con
                    void* stream, int host_checks);
 
 /*
+ * Batched CG (no counterpart in the reference, which solves one mesh at a time): a
+ * block-diagonal system of n_seg independent segments (the meshes of a batch stored back
+ * to back; segment s owns unknowns seg_offsets[s] .. seg_offsets[s+1], whole nodes) is
+ * solved as n_seg independent preconditioned CGs run in the same launches, each with its
+ * own step lengths, residual test max(atol, rtol ||b_s||) and iteration count, so every
+ * instance converges at its own rate.  precond must be PSX_PRECOND_BJACOBI (optionally |
+ * PSX_PCG_NODAL); coarse (or NULL) adds the two-level correction.  seg_offsets (int64,
+ * n_seg + 1) and node_seg (int32, N: segment of each node) on the device.  Exactly
+ * maxiter iterations are enqueued (finished segments stop updating), nothing is read
+ * back.  status: iters = most iterations of a segment, flags = 0 if every segment
+ * converged (2: a segment hit maxiter, 4: a breakdown); seg_iters (device, n_seg, or
+ * NULL) receives each segment's iterations, as -(iterations + 1) if it did not converge.
+ * Workspace: psx_pcg_batched_work_bytes.
+ */
+int psx_pcg_batched_work_bytes(int64_t n, int32_t n_seg, int64_t* bytes);
+int psx_pcg_batched(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                    int value_precision, const double* b, double* x, double rtol, double atol, int32_t maxiter,
+                    int precond, int32_t n_seg, const int64_t* seg_offsets, const int32_t* node_seg,
+                    const psx_coarse_t* coarse, void* work, int64_t work_bytes, void* status, int32_t* seg_iters,
+                    void* stream);
+
+/*
  * y = alpha A x + beta y for a CSR matrix (values double for PSX_FP64, float for
  * PSX_FP32_MIXED; x, y double, device), rows summed in a fixed order: the products with
  * the constant mass and stiffness matrices in the dynamic residual

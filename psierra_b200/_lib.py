@@ -84,6 +84,9 @@ SIGNATURES: dict[str, list] = {
     "psx_coarse_probe": [_p, _p, _i32, _i32, _p, _p],
     "psx_coarse_restrict": [_p, _p, _p, _p],
     "psx_pcg_coarse": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _p, _p, _i64, _p, _p, _i32],
+    "psx_pcg_batched_work_bytes": [_i64, _i32, _p],
+    "psx_pcg_batched": [_i64, _p, _p, _p, _i32, _p, _p, _f64, _f64, _i32, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p,
+                        _p],
 }
 
 

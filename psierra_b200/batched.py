@@ -17,16 +17,20 @@ iteration for the whole batch is one replay of a captured CUDA graph:
   coarse correction of ``psierra_b200.coarse``, whose coarse matrices are refreshed from
   the new tangent inside the same replay) -> du_i = ref_i * solution -> u += du.
 
-The system is block diagonal, so scaling instance i's right-hand side by 1/ref_i
-(ref_i = ||lambda f_ext,i||) scales only that instance's solution: every instance gets
-the same relative CG accuracy from the one global stopping test.  An instance that has
-converged (or failed) gets a zero right-hand side, and CG then leaves its block of the
-solution exactly zero, so it stays frozen as the reference's loop would leave it.  An
-instance whose residual turns non-finite (an inverted element) is retired like a
-non-converged one.  The host reads the B residual norms once per replay to decide
-convergence; nothing else leaves the device.  Steps are taken in full (no line
-search), and a non-converged instance keeps its last converged load step, as
-``NonlinearStaticAnalysis`` returns it.
+The system is block diagonal.  By default it is solved as one independent CG per
+instance in the same launches (``psx_pcg_batched``: per-instance step lengths, residual
+test and iteration count), so each instance converges at its own rate; one CG over the
+whole system (``per_instance_cg=False``) shares its step lengths and converges at the rate
+of the worst-conditioned instance.  Instance i's right-hand side is scaled by 1/ref_i
+(ref_i = ||lambda f_ext,i||), which gives every instance the same relative accuracy in
+the shared CG as well.  An instance that has converged (or failed) gets a zero
+right-hand side, and CG then leaves its block of the solution exactly zero, so it stays
+frozen as the reference's loop would leave it.  The host reads the B residual norms
+once per replay to decide convergence; nothing else leaves the device.  Each replay is
+also a trial: an instance whose residual turned non-finite (an inverted element) or grew
+more than a hundredfold goes back to half of its step, as the reference's line search
+contracts on inversion (``analysis/line_search.py:120-260``).  A non-converged instance keeps its last
+converged load step, as ``NonlinearStaticAnalysis`` returns it.
 """
 from __future__ import annotations
 
@@ -123,10 +127,15 @@ class BatchedNewtonResult:
 class BatchedNewton:
     def __init__(self, batch: MeshBatch, fixed_dofs, precision: str | None = None, pcg_iterations: int = 500,
                  pcg_rtol: float = 1e-8, preconditioner: str = "block-jacobi", use_graph: bool = True,
-                 nodes_per_aggregate: int = 500):
+                 levels_per_aggregate: int = 4, per_instance_cg: bool = True):
         """``fixed_dofs``: per instance, its clamped DOFs in local numbering.
         ``preconditioner``: "none", "jacobi", "block-jacobi" or "two-level" (block-Jacobi
-        plus rigid-body modes of slices of about ``nodes_per_aggregate`` nodes)."""
+        plus rigid-body modes of slices of about ``levels_per_aggregate`` cross-sections).
+        ``per_instance_cg``: run one CG per instance (own step lengths and residual test,
+        ``psx_pcg_batched``) instead of one CG over the whole block-diagonal system; with
+        the shared step lengths of the latter every instance converges at the rate of the
+        worst-conditioned one (block-Jacobi and two-level; the plain Jacobi and
+        unpreconditioned options always use one CG)."""
         self.batch = batch
         asm = batch.asm
         self.asm = asm
@@ -152,7 +161,7 @@ class BatchedNewton:
             from psierra_b200.coarse import CoarseSpace
 
             self.coarse = CoarseSpace(batch.mesh.nodes, batch.mesh.elements, mask, batch.node_offsets,
-                                      nodes_per_aggregate, device=dev)
+                                      levels_per_aggregate, device=dev)
         self.use_graph = use_graph
         f64 = dict(dtype=torch.float64, device=dev)
         B = batch.B
@@ -170,8 +179,16 @@ class BatchedNewton:
         self.tol2 = torch.full((B,), float("inf"), **f64)
         self.act_b = torch.zeros(B, dtype=torch.bool, device=dev)
         self.act_f = torch.zeros(B, **f64)
+        self._zero = torch.zeros((), **f64)
+        self.per_instance_cg = per_instance_cg and preconditioner in ("block-jacobi", "two-level")
         nb = ctypes.c_int64()
-        check(lib().psx_pcg_work_bytes(n, self.precond, ctypes.byref(nb)), "psx_pcg_work_bytes")
+        if self.per_instance_cg:
+            check(lib().psx_pcg_batched_work_bytes(n, B, ctypes.byref(nb)), "psx_pcg_batched_work_bytes")
+            self.node_seg = torch.from_numpy(np.repeat(np.arange(B, dtype=np.int32),
+                                                       np.diff(batch.node_offsets))).to(dev)
+            self.seg_iters = torch.zeros(B, dtype=torch.int32, device=dev)
+        else:
+            check(lib().psx_pcg_work_bytes(n, self.precond, ctypes.byref(nb)), "psx_pcg_work_bytes")
         self.pcg_work = torch.empty(int(nb.value), dtype=torch.uint8, device=dev)
         self.pcg_status = torch.zeros((int(lib().psx_status_bytes()) + 3) // 4, dtype=torch.int32, device=dev)
         self._graph: torch.cuda.CUDAGraph | None = None
@@ -190,11 +207,22 @@ class BatchedNewton:
         torch.ge(self.rn2, self.tol2, out=self.act_b)
         self.act_f.copy_(self.act_b)
         torch.index_select(self.act_f, 0, self.batch.dof_instance, out=self.act_dof)
+        # inactive instances get an exactly zero right-hand side (a where, not a product: a
+        # retired instance's residual may be NaN, and NaN * 0 would reach every instance
+        # through the CG's shared step lengths)
         torch.mul(self.r, self.inv_scale, out=self.rhs)
-        self.rhs.mul_(self.act_dof)
+        torch.where(self.act_dof > 0, self.rhs, self._zero, out=self.rhs)
         self.du.zero_()
         if self.coarse is not None:
             self.coarse.update(self.k, d["indptr"], d["indices"])
+        if self.per_instance_cg:
+            check(lib().psx_pcg_batched(self.n, ptr(d["indptr"]), ptr(d["indices"]), ptr(self.k), vp, ptr(self.rhs),
+                                        ptr(self.du), self.pcg_rtol, 0.0, self.pcg_iterations, self.precond,
+                                        self.batch.B, ptr(self.batch.dof_offsets_dev), ptr(self.node_seg),
+                                        self.coarse.struct_ptr() if self.coarse is not None else None,
+                                        ptr(self.pcg_work), self.pcg_work.numel(), ptr(self.pcg_status),
+                                        ptr(self.seg_iters), _stream()), "psx_pcg_batched")
+        elif self.coarse is not None:
             check(lib().psx_pcg_coarse(self.n, ptr(d["indptr"]), ptr(d["indices"]), ptr(self.k), vp, ptr(self.rhs),
                                        ptr(self.du), self.pcg_rtol, 0.0, self.pcg_iterations, self.precond,
                                        self.coarse.struct_ptr(), ptr(self.pcg_work), self.pcg_work.numel(),
@@ -234,13 +262,26 @@ class BatchedNewton:
 
     # ------------------------------------------------------------------ driver
     def solve(self, f_ext: torch.Tensor, n_steps: int = 8, nr_iterations: int = 25,
-              nr_tol: float = 1e-8) -> BatchedNewtonResult:
+              nr_tol: float = 1e-8, max_halvings: int = 16, max_growth: float = 100.0) -> BatchedNewtonResult:
+        """Incremental Newton of every instance with full steps and a divergence guard:
+        a trial point is rejected, and its step length alpha halved, when its residual is
+        non-finite (an inverted element) or more than ``max_growth`` times the residual
+        at the last accepted point.  (The reference's line search, analysis/line_search.py:
+        120-260, also rejects moderate growth; measured on the 256-beam batch that cuts the
+        steps of instances that converge quadratically after one larger residual: 175 of
+        256 converged in 585 replays, against 256 with this guard.)  Every trial is one
+        replay; an instance gives up after ``max_halvings`` halvings of one step or
+        ``nr_iterations`` accepted Newton iterations, and is then retired at its last
+        converged load step."""
         b = self.batch
         B = b.B
         dev = self.asm.device
         f_ext = f_ext.to(dev, torch.float64)
+        counts = np.diff(b.dof_offsets)
+        dofs = lambda mask: torch.from_numpy(np.repeat(mask, counts)).to(dev)  # noqa: E731
         self.u.zero_()
         u_acc = self.u.clone()
+        direction = torch.zeros_like(self.u)  # each instance's Newton step from its accepted point
         alive = np.ones(B, dtype=bool)
         steps_done = np.zeros(B, dtype=np.int64)
         its = np.zeros((n_steps, B), dtype=np.int64)
@@ -260,27 +301,51 @@ class BatchedNewton:
             torch.index_select(torch.from_numpy(ref).to(dev), 0, b.dof_instance, out=self.scale)
             torch.reciprocal(self.scale, out=self.inv_scale)
             conv = ~alive  # retired instances take no part
-            for it in range(1, nr_iterations + 1):
+            accepted = np.zeros(B, dtype=np.int64)  # accepted points (the start counts)
+            rn_acc = np.full(B, np.inf)  # residual at the last accepted point
+            alpha = np.ones(B)
+            direction.zero_()
+            for _ in range(4 * nr_iterations):
                 self.iterate()
                 replays += 1
-                # an inverted element makes its instance's residual non-finite (ln J of
-                # J <= 0), which retires that instance below
-                rn2 = self.rn2.cpu().numpy()
+                rn = np.sqrt(self.rn2.cpu().numpy())
                 # the replay assembled with check_status=False: a bounded wait that gave
                 # up leaves a K_T summed out of order, so no instance may use this step
                 raise_if_wait_gave_up(self.asm.status_counts()[3])
-                hist.append(np.sqrt(rn2))
-                newly = alive & ~conv & (rn2 < tol * tol)  # the device's test, negated
-                its[step - 1, newly] = it
-                bad = alive & ~conv & ~np.isfinite(rn2)
+                hist.append(rn)
+                active = alive & ~conv
+                with np.errstate(invalid="ignore"):
+                    ok = np.isfinite(rn) & ((accepted == 0) | (rn < tol) | (rn <= max_growth * rn_acc))
+                acc = active & ok
+                rej = active & ~ok
+                accepted[acc] += 1
+                rn_acc[acc] = rn[acc]
+                alpha[acc] = 1.0
+                newly = acc & (rn < tol)  # the device's test (it gave them no step)
+                its[step - 1, newly] = accepted[newly]
+                # the replay also took a full step from every trial point: the accepted
+                # ones keep it as their new direction; the rejected ones go back from
+                # their trial point (accepted point + alpha direction) to alpha / 2
+                if rej.any():
+                    m = dofs(rej)
+                    back = torch.where(m, self.du + (0.5 * torch.from_numpy(np.repeat(alpha, counts)).to(dev)) * direction,
+                                       self._zero)
+                    self.u.sub_(back)
+                    alpha[rej] *= 0.5
+                torch.where(dofs(acc), self.du, direction, out=direction)
+                bad = (rej & (alpha < 0.5 ** max_halvings)) | (active & (accepted > nr_iterations) & ~newly)
                 alive &= ~bad
                 conv |= newly | bad
+                if bad.any():
+                    # back to its last converged state: a non-finite u would make its
+                    # tangent block non-finite
+                    torch.where(dofs(bad), u_acc, self.u, out=self.u)
                 if conv.all():
                     break
                 # freeze the instances that are done
                 self.tol2.copy_(torch.from_numpy(np.where(conv, np.inf, tol * tol)))
-            alive &= conv  # not converged within nr_iterations: retired at its last step
-            keep = torch.from_numpy(np.repeat(alive, np.diff(b.dof_offsets))).to(dev)
+            alive &= conv  # not converged: retired at its last step
+            keep = dofs(alive)
             u_acc = torch.where(keep, self.u, u_acc)
             self.u.copy_(u_acc)
             steps_done[alive] = step

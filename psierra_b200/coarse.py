@@ -11,8 +11,9 @@ correction of a two-level additive Schwarz method:
 with B the node blocks of A and P six columns per aggregate of nodes (three
 translations, three rotations about the aggregate's centroid: a rigid motion of the
 aggregate).  Aggregates are slices of each mesh instance along its longest principal
-axis, about ``nodes_per_aggregate`` nodes each, so that a beam's coarse space carries its
-bending and torsion, which block-Jacobi resolves slowest.
+axis, a few cross-sections each (sized by positions along the axis, not by node count, so
+that a thin beam gets as many slices as a thick one), so that a beam's coarse space
+carries its bending and torsion, which block-Jacobi resolves slowest.
 
 A_c changes with every tangent.  It is assembled on the device by probing: the
 aggregates are coloured so that two aggregates of one colour are never both coupled to a
@@ -33,11 +34,13 @@ import torch
 from psierra_b200._lib import CoarseStruct, check, lib, ptr
 
 
-def slice_aggregates(nodes: np.ndarray, node_offsets, nodes_per_aggregate: int = 500):
+def slice_aggregates(nodes: np.ndarray, node_offsets, levels_per_aggregate: int = 4, max_aggregates: int = 64):
     """Aggregate of every node: per instance (nodes node_offsets[i]:node_offsets[i+1]),
-    slices of roughly equal node count along the instance's longest principal axis.
-    Nodes with the same coordinate along the axis share a slice.  Returns (node_agg (N,),
-    block_agg (B+1,)), aggregates numbered instance by instance."""
+    slices of roughly equal node count along the instance's longest principal axis, each
+    about ``levels_per_aggregate`` distinct positions along it (cross-sections of a
+    structured mesh), at most ``max_aggregates`` per instance.  Nodes with the same
+    coordinate along the axis share a slice.  Returns (node_agg (N,), block_agg (B+1,)),
+    aggregates numbered instance by instance."""
     X = np.asarray(nodes, dtype=np.float64)
     offs = np.asarray(node_offsets, dtype=np.int64)
     node_agg = np.empty(X.shape[0], dtype=np.int64)
@@ -52,7 +55,7 @@ def slice_aggregates(nodes: np.ndarray, node_offsets, nodes_per_aggregate: int =
         span = max(float(np.ptp(t)), 1e-300)
         levels, inv, counts = np.unique(np.round(t / (1e-9 * span)), return_inverse=True, return_counts=True)
         n = hi - lo
-        n_agg = max(1, int(round(n / max(1, nodes_per_aggregate))))
+        n_agg = min(max_aggregates, max(1, int(round(len(levels) / max(1, levels_per_aggregate)))))
         mid = np.cumsum(counts) - 0.5 * counts  # node rank at the middle of each level
         level_agg = np.minimum((mid * n_agg / n).astype(np.int64), n_agg - 1)
         used, a = np.unique(level_agg[inv], return_inverse=True)  # drop empty slices
@@ -105,12 +108,12 @@ class CoarseSpace:
     ``struct`` is the ``psx_coarse_t`` the CG takes.
     """
 
-    def __init__(self, nodes, elements, fixed, node_offsets=None, nodes_per_aggregate: int = 500,
-                 device=None) -> None:
+    def __init__(self, nodes, elements, fixed, node_offsets=None, levels_per_aggregate: int = 4,
+                 max_aggregates: int = 64, device=None) -> None:
         X = np.asarray(nodes, dtype=np.float64)
         N = X.shape[0]
         offs = np.asarray([0, N] if node_offsets is None else node_offsets, dtype=np.int64)
-        node_agg, block_agg = slice_aggregates(X, offs, nodes_per_aggregate)
+        node_agg, block_agg = slice_aggregates(X, offs, levels_per_aggregate, max_aggregates)
         n_agg = int(block_agg[-1])
         order = np.argsort(node_agg, kind="stable")
         agg_ptr = np.searchsorted(node_agg[order], np.arange(n_agg + 1))
@@ -236,6 +239,7 @@ class CoarseSpace:
         torch.bmm(Li.transpose(1, 2), Li, out=self.ainv)
         # a block whose A_c is not positive definite (a tangent that lost definiteness)
         # gets no coarse correction: that instance runs plain block-Jacobi
-        ok = (info == 0).to(a.dtype)
-        self.ainv.mul_(keep[:, :, None] * keep[:, None, :] * ok[:, None, None])
+        # (a failed factor may hold NaN, which a multiplication by zero would keep)
+        use = (keep[:, :, None] * keep[:, None, :] > 0) & (info == 0)[:, None, None]
+        torch.where(use, self.ainv, torch.zeros((), dtype=a.dtype, device=a.device), out=self.ainv)
         self.factor_ok = info == 0

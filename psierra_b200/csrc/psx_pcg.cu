@@ -630,6 +630,190 @@ bool coarse_ok(const psx_coarse_t* c) {
          c->n_blocks > 0 && c->nc > 0 && c->nc <= kCoarseMaxNc && c->block_agg && c->ainv && c->rc && c->yc;
 }
 
+// ---- batched CG: one independent CG per segment of a block-diagonal system -----------
+// The unknowns of segment s are [off[s], off[s+1]) (whole nodes); each segment has its
+// own step lengths, residual test and iteration count, so a batch of meshes solved as
+// one system converges instance by instance, at each instance's own rate, instead of
+// at the rate of the worst-conditioned instance (which shared step lengths give).  The
+// per-segment dot products are reduced by one thread block per segment in a fixed
+// order.
+struct SegScalars {
+  double rho, rho_prev, alpha, rr, bb, atol2;
+  int32_t state;  // 0 running, 1 converged, 2 iteration limit, 4 breakdown
+  int32_t iters, first, pad;
+};
+
+struct BatchArgs {
+  int32_t n_seg;
+  const int64_t* off;     // n_seg + 1 unknown offsets (multiples of 3)
+  const int32_t* node_seg;  // segment of each node
+  SegScalars* seg;
+};
+
+// z = B^-1 r (+ P yc) for every node of a running segment
+template <bool COARSE>
+__global__ void __launch_bounds__(kBlock) bpcg_precond(int64_t n, PcgWork w, BatchArgs ba, psx_coarse_t c) {
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n / 3; i += (int64_t)gridDim.x * kBlock) {
+    if (ba.seg[ba.node_seg[i]].state) continue;
+    apply_prec<true>(w, i, w.z, w.r);
+    if constexpr (COARSE) {
+      const int32_t a = c.node_agg[i];
+      if (a >= 0) {
+        const double* y = c.yc + 6 * (int64_t)a;
+        const double dx = c.d[3 * i], dy = c.d[3 * i + 1], dz = c.d[3 * i + 2];
+        const double add[3] = {y[0] + (y[4] * dz - y[5] * dy), y[1] + (y[5] * dx - y[3] * dz),
+                               y[2] + (y[3] * dy - y[4] * dx)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          if (!c.fixed[3 * i + k]) w.z[3 * i + k] += add[k];
+      }
+    }
+  }
+}
+
+// Per-segment dot products, one block per segment.  KIND 0: initial (r.r, r.z, b.b);
+// 1: p.q -> alpha; 2: (r.r, r.z) -> the next iteration's scalars and the residual test.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) bpcg_segdots(const double* __restrict__ b, PcgWork w, BatchArgs ba,
+                                                        double rtol, double atol, int32_t maxiter) {
+  SegScalars* s = ba.seg + blockIdx.x;
+  if (KIND != 0 && s->state) return;
+  const int64_t d0 = ba.off[blockIdx.x], d1 = ba.off[blockIdx.x + 1];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int64_t d = d0 + threadIdx.x; d < d1; d += kBlock) {
+    if constexpr (KIND == 1) {
+      v[0] += w.p[d] * w.q[d];
+    } else {
+      v[0] += w.r[d] * w.r[d];
+      v[1] += w.r[d] * w.z[d];
+      if constexpr (KIND == 0) v[2] += b[d] * b[d];
+    }
+  }
+  block_sum<3>(v);
+  if (threadIdx.x != 0) return;
+  if constexpr (KIND == 0) {
+    s->rr = v[0];
+    s->rho = v[1];
+    s->bb = v[2];
+    const double a = fmax(atol, rtol * sqrt(v[2]));
+    s->atol2 = a * a;
+    s->iters = 0;
+    s->first = 1;
+    s->state = (v[2] == 0.0 || sqrt(v[0]) < a) ? 1 : 0;
+  } else if constexpr (KIND == 1) {
+    if (!(v[0] != 0.0) || !isfinite(v[0])) {
+      s->state = 4;
+      s->alpha = 0.0;
+    } else {
+      s->alpha = s->rho / v[0];
+    }
+  } else {
+    s->rho_prev = s->rho;
+    s->rr = v[0];
+    s->rho = v[1];
+    s->first = 0;
+    s->iters += 1;
+    if (!isfinite(v[0])) s->state = 4;
+    else if (v[0] < s->atol2) s->state = 1;
+    else if (s->iters >= maxiter) s->state = 2;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) bpcg_update_p(int64_t n, PcgWork w, BatchArgs ba) {
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+    const SegScalars* s = ba.seg + ba.node_seg[i / 3];
+    if (s->state) continue;
+    w.p[i] = s->first ? w.z[i] : w.z[i] + (s->rho / s->rho_prev) * w.p[i];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) bpcg_update_xr(int64_t n, double* __restrict__ x, PcgWork w, BatchArgs ba) {
+  for (int64_t i = blockIdx.x * (int64_t)kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+    const SegScalars* s = ba.seg + ba.node_seg[i / 3];
+    if (s->state) continue;
+    x[i] += s->alpha * w.p[i];
+    w.r[i] -= s->alpha * w.q[i];
+  }
+}
+
+// q = A p over the whole system (the blocks of finished segments compute on a frozen p)
+template <typename VT, bool NODAL>
+__global__ void __launch_bounds__(kBlock) bpcg_spmv(int64_t n, const int32_t* __restrict__ indptr,
+                                                    const int32_t* __restrict__ indices, const VT* __restrict__ vals,
+                                                    PcgWork w) {
+  if constexpr (NODAL) {
+    const int lane16 = threadIdx.x & (kNodeLanes - 1);
+    const int64_t nodes = n / 3, per_pass = (int64_t)gridDim.x * (kBlock / kNodeLanes);
+    for (int64_t node0 = blockIdx.x * (int64_t)(kBlock / kNodeLanes); node0 < nodes; node0 += per_pass) {
+      const int64_t node = node0 + threadIdx.x / kNodeLanes;
+      double q[3];
+      spmv_node<VT>(nodes, node, lane16, indptr, indices, vals, w.p, q);
+      if (node < nodes && lane16 == 0)
+        for (int k = 0; k < 3; ++k) w.q[3 * node + k] = q[k];
+    }
+  } else {
+    const int lane8 = threadIdx.x & (kRowLanes - 1);
+    const int64_t rows_per_pass = (int64_t)gridDim.x * (kBlock / kRowLanes);
+    for (int64_t row0 = blockIdx.x * (int64_t)(kBlock / kRowLanes); row0 < n; row0 += rows_per_pass) {
+      const int64_t row = row0 + threadIdx.x / kRowLanes;
+      const double q = spmv_row<VT>(n, row, lane8, indptr, indices, vals, w.p);
+      if (row < n && lane8 == 0) w.q[row] = q;
+    }
+  }
+}
+
+__global__ void bpcg_report(BatchArgs ba, Status* st, int32_t* seg_iters) {
+  int32_t most = 0, flags = 0;
+  double rr = 0.0;
+  for (int32_t s = 0; s < ba.n_seg; ++s) {
+    const SegScalars& g = ba.seg[s];
+    most = max(most, g.iters);
+    if (g.state != 1) flags |= g.state == 2 ? 2 : 4;
+    rr += g.rr;
+    if (seg_iters) seg_iters[s] = g.state == 1 ? g.iters : -g.iters - 1;
+  }
+  st->iters = most;
+  st->flags = flags;
+  st->value = sqrt(rr);
+}
+
+template <typename VT, bool NODAL, bool COARSE>
+int run_pcg_batched(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* vals, const double* b,
+                    double* x, double rtol, double atol, int32_t maxiter, const PcgWork& w, const BatchArgs& ba,
+                    const psx_coarse_t& c, Status* st, int32_t* seg_iters, cudaStream_t s) {
+  const int grid_vec = (int)std::min<int64_t>(kGridMax, (n + kBlock - 1) / kBlock);
+  const int grid_nodes = (int)std::min<int64_t>(kGridMax, (n / 3 + kBlock - 1) / kBlock);
+  const int grid_row = NODAL ? (int)std::min<int64_t>(kGridMax, (n / 3 + kBlock / kNodeLanes - 1) / (kBlock / kNodeLanes))
+                             : (int)std::min<int64_t>(kGridMax, (n + kBlock / kRowLanes - 1) / (kBlock / kRowLanes));
+  const int grid_agg = COARSE ? (int)std::min<int64_t>(kGridMax, (c.n_agg + kBlock / 32 - 1) / (kBlock / 32)) : 1;
+  const size_t smem = COARSE ? sizeof(double) * (size_t)c.nc : 0;
+  if (cudaMemsetAsync(ba.seg, 0, sizeof(SegScalars) * ba.n_seg, s) != cudaSuccess) return PSX_ERR_CUDA;
+  bjacobi_setup<<<grid_vec, kBlock, 0, s>>>(n / 3, indptr, indices, vals, sizeof(VT) == 4, w.minv, w.s);
+  pcg_init_residual<VT, true, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, b, x, w);
+  auto precond = [&]() {
+    if constexpr (COARSE) {
+      coarse_restrict_kernel<<<grid_agg, kBlock, 0, s>>>(c, w.r, c.rc, nullptr);
+      coarse_gemv_kernel<<<c.n_blocks, kBlock, smem, s>>>(c, nullptr);
+    }
+    bpcg_precond<COARSE><<<grid_nodes, kBlock, 0, s>>>(n, w, ba, c);
+  };
+  precond();
+  bpcg_segdots<0><<<ba.n_seg, kBlock, 0, s>>>(b, w, ba, rtol, atol, maxiter);
+  PSX_CUDA_CHECK_LAUNCH();
+  for (int32_t k = 0; k < maxiter; ++k) {
+    bpcg_update_p<<<grid_vec, kBlock, 0, s>>>(n, w, ba);
+    bpcg_spmv<VT, NODAL><<<grid_row, kBlock, 0, s>>>(n, indptr, indices, vals, w);
+    bpcg_segdots<1><<<ba.n_seg, kBlock, 0, s>>>(b, w, ba, rtol, atol, maxiter);
+    bpcg_update_xr<<<grid_vec, kBlock, 0, s>>>(n, x, w, ba);
+    precond();
+    bpcg_segdots<2><<<ba.n_seg, kBlock, 0, s>>>(b, w, ba, rtol, atol, maxiter);
+    if ((k & 15) == 15) PSX_CUDA_CHECK_LAUNCH();
+  }
+  bpcg_report<<<1, 1, 0, s>>>(ba, st, seg_iters);
+  PSX_CUDA_CHECK_LAUNCH();
+  return PSX_OK;
+}
+
 }  // namespace
 }  // namespace psx
 
@@ -708,6 +892,52 @@ extern "C" int psx_pcg_coarse(int64_t n, const int32_t* indptr, const int32_t* i
   const float* v = static_cast<const float*>(values);
   return nodal ? run_pcg_coarse<float, true>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc)
                : run_pcg_coarse<float, false>(n, indptr, indices, v, b, x, rtol, atol, maxiter, w, *coarse, st, s, hc);
+}
+
+extern "C" int psx_pcg_batched_work_bytes(int64_t n, int32_t n_seg, int64_t* bytes) {
+  using namespace psx;
+  if (n <= 0 || n % 3 || n_seg <= 0 || !bytes) return PSX_ERR_ARG;
+  PcgWork w;
+  int64_t vec = 0;
+  layout(n, PSX_PRECOND_BJACOBI, nullptr, &w, &vec);
+  *bytes = vec + (int64_t)up256(sizeof(SegScalars) * (size_t)n_seg);
+  return PSX_OK;
+}
+
+extern "C" int psx_pcg_batched(int64_t n, const int32_t* indptr, const int32_t* indices, const void* values,
+                               int value_precision, const double* b, double* x, double rtol, double atol,
+                               int32_t maxiter, int precond, int32_t n_seg, const int64_t* seg_offsets,
+                               const int32_t* node_seg, const psx_coarse_t* coarse, void* work, int64_t work_bytes,
+                               void* status, int32_t* seg_iters, void* stream) {
+  using namespace psx;
+  if (n <= 0 || !indptr || !indices || !values || !b || !x || !work || !status || maxiter < 0 || n_seg <= 0 ||
+      !seg_offsets || !node_seg)
+    return PSX_ERR_ARG;
+  const bool nodal = (precond & PSX_PCG_NODAL) != 0;
+  if ((precond & ~PSX_PCG_NODAL) != PSX_PRECOND_BJACOBI || n % 3) return PSX_ERR_ARG;
+  if (coarse && (!coarse_ok(coarse) || coarse->n_nodes * 3 != n))
+    return coarse->nc > kCoarseMaxNc ? PSX_ERR_LIMIT : PSX_ERR_ARG;
+  if (value_precision != PSX_FP64 && value_precision != PSX_FP32_MIXED) return PSX_ERR_ARG;
+  int64_t need = 0;
+  if (psx_pcg_batched_work_bytes(n, n_seg, &need) != PSX_OK || work_bytes < need) return PSX_ERR_ARG;
+  PcgWork w;
+  int64_t vec = 0;
+  int rc = layout(n, PSX_PRECOND_BJACOBI, work, &w, &vec);
+  if (rc != PSX_OK) return rc;
+  BatchArgs ba{n_seg, seg_offsets, node_seg, reinterpret_cast<SegScalars*>(static_cast<char*>(work) + vec)};
+  const psx_coarse_t c = coarse ? *coarse : psx_coarse_t{};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Status* st = static_cast<Status*>(status);
+#define PSX_RUN(VT, NOD, CO)                                                                                        \
+  run_pcg_batched<VT, NOD, CO>(n, indptr, indices, static_cast<const VT*>(values), b, x, rtol, atol, maxiter, w, ba, \
+                               c, st, seg_iters, s)
+  if (value_precision == PSX_FP64) {
+    if (nodal) return coarse ? PSX_RUN(double, true, true) : PSX_RUN(double, true, false);
+    return coarse ? PSX_RUN(double, false, true) : PSX_RUN(double, false, false);
+  }
+  if (nodal) return coarse ? PSX_RUN(float, true, true) : PSX_RUN(float, true, false);
+  return coarse ? PSX_RUN(float, false, true) : PSX_RUN(float, false, false);
+#undef PSX_RUN
 }
 
 extern "C" int psx_coarse_probe(const psx_coarse_t* coarse, const int32_t* agg_color, int32_t color, int32_t mode,

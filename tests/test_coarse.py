@@ -41,7 +41,7 @@ def _dense_P(X, node_agg, fixed, n_agg):
 
 def test_slices_follow_the_long_axis_and_colouring_is_distance_two():
     meshes, union, node_off = _beams()
-    node_agg, block_agg = slice_aggregates(union.nodes, node_off, nodes_per_aggregate=32)
+    node_agg, block_agg = slice_aggregates(union.nodes, node_off, levels_per_aggregate=2)
     assert block_agg[0] == 0 and np.all(np.diff(block_agg) > 1)
     for b, m in enumerate(meshes):
         agg = node_agg[node_off[b]:node_off[b + 1]]
@@ -72,7 +72,7 @@ def test_probing_assembles_P_T_A_P_and_the_preconditioner_matches_its_definition
     # symmetric elimination, as psx_csr_dirichlet does it
     keep = sp.diags((fixed == 0).astype(float))
     K = (keep @ K @ keep + sp.diags(fixed.astype(float))).tocsr()
-    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, nodes_per_aggregate=32, device="cpu")
+    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, levels_per_aggregate=2, device="cpu")
     node_agg = cs.node_agg.numpy().astype(np.int64)
     P = _dense_P(union.nodes, node_agg, fixed, cs.n_agg)
     colour = cs.agg_colour.numpy()

@@ -54,7 +54,7 @@ def _eliminated_tangent(asm, fixed, precision):
 
 def test_probe_and_restrict_kernels_match_dense_P():
     meshes, union, node_off, asm, fixed = _two_beams()
-    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, nodes_per_aggregate=64)
+    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, levels_per_aggregate=4)
     P = _dense_P(union.nodes, cs.node_agg.cpu().numpy().astype(np.int64), fixed, cs.n_agg)
     colour = cs.agg_colour.cpu().numpy()
     v = torch.empty(3 * union.n_nodes, dtype=torch.float64, device=DEV)
@@ -76,7 +76,7 @@ def test_coarse_matrix_is_P_T_K_P(precision):
 
     meshes, union, node_off, asm, fixed = _two_beams(precision)
     k = _eliminated_tangent(asm, fixed, precision)
-    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, nodes_per_aggregate=64)
+    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, levels_per_aggregate=4)
     cs.update(k, asm.dev["indptr"], asm.dev["indices"])
     n = 3 * union.n_nodes
     K = sp.csr_matrix((k.double().cpu().numpy(), asm.pattern.indices, asm.pattern.indptr), shape=(n, n))
@@ -98,7 +98,7 @@ def test_two_level_cg_matches_block_jacobi_in_far_fewer_iterations():
     f = np.concatenate([meshgen.traction_nodal_forces(m, int(np.argmax(np.ptp(m.nodes, axis=0))), "max",
                                                       [0.0, 0.0, -10.0]) for m in meshes])
     b = torch.from_numpy(f * (fixed == 0)).to(DEV)
-    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, nodes_per_aggregate=64)
+    cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, levels_per_aggregate=4)
     cs.update(k, d["indptr"], d["indices"])
     prec = _lib.PSX_PRECOND_BJACOBI | _lib.PSX_PCG_NODAL
     nb = ctypes.c_int64()
@@ -130,8 +130,54 @@ def test_batched_newton_two_level_matches_block_jacobi():
     res = {}
     for name, its in (("block-jacobi", 3000), ("two-level", 300)):
         bn = BatchedNewton(mb, [c[4] for c in cases], pcg_iterations=its, pcg_rtol=1e-10, preconditioner=name,
-                           nodes_per_aggregate=24)
+                           levels_per_aggregate=2)
         res[name] = bn.solve(f, n_steps=3, nr_iterations=25, nr_tol=1e-8)
         assert res[name].converged.all(), name
     for a, b in zip(res["two-level"].u, res["block-jacobi"].u):
         assert rel_2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("coarse", [False, True])
+def test_batched_cg_solves_each_instance_like_its_own_cg(coarse):
+    """psx_pcg_batched: one CG per segment of a block-diagonal system; each segment's
+    solution equals that instance's own solve (psx_pcg, block-Jacobi) to the solver
+    tolerance, and the segments converge with their own iteration counts."""
+    meshes, union, node_off, asm, fixed = _two_beams()
+    k = _eliminated_tangent(asm, fixed, "fp64")
+    d = asm.dev
+    n = 3 * union.n_nodes
+    f = np.concatenate([meshgen.traction_nodal_forces(m, int(np.argmax(np.ptp(m.nodes, axis=0))), "max",
+                                                      [0.0, 0.0, -10.0 * (1 + 99 * b)]) for b, m in enumerate(meshes)])
+    b = torch.from_numpy(f * (fixed == 0)).to(DEV)
+    prec = _lib.PSX_PRECOND_BJACOBI | _lib.PSX_PCG_NODAL
+    B = len(meshes)
+    seg_off = torch.from_numpy(3 * np.asarray(node_off, dtype=np.int64)).to(DEV)
+    node_seg = torch.from_numpy(np.repeat(np.arange(B, dtype=np.int32), np.diff(node_off))).to(DEV)
+    cs = None
+    if coarse:
+        cs = CoarseSpace(union.nodes, union.elements, fixed, node_off, levels_per_aggregate=4)
+        cs.update(k, d["indptr"], d["indices"])
+    nb = ctypes.c_int64()
+    check(lib().psx_pcg_batched_work_bytes(n, B, ctypes.byref(nb)), "psx_pcg_batched_work_bytes")
+    work = torch.empty(int(nb.value), dtype=torch.uint8, device=DEV)
+    st = torch.zeros((int(lib().psx_status_bytes()) + 3) // 4, dtype=torch.int32, device=DEV)
+    seg_iters = torch.zeros(B, dtype=torch.int32, device=DEV)
+    x = torch.zeros(n, dtype=torch.float64, device=DEV)
+    check(lib().psx_pcg_batched(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), _lib.PSX_FP64, ptr(b), ptr(x), 1e-12,
+                                0.0, 20000, prec, B, ptr(seg_off), ptr(node_seg),
+                                cs.struct_ptr() if cs is not None else None, ptr(work), work.numel(), ptr(st),
+                                ptr(seg_iters), _stream()), "psx_pcg_batched")
+    its = seg_iters.cpu().numpy()
+    assert (its > 0).all() and st.cpu().numpy()[5] == 0, (its, st.cpu().numpy())
+    # reference: each instance alone (block-Jacobi CG on its own block of the system)
+    check(lib().psx_pcg_work_bytes(n, prec, ctypes.byref(nb)), "psx_pcg_work_bytes")
+    work1 = torch.empty(int(nb.value), dtype=torch.uint8, device=DEV)
+    for s in range(B):
+        bs = torch.zeros_like(b)
+        lo, hi = 3 * int(node_off[s]), 3 * int(node_off[s + 1])
+        bs[lo:hi] = b[lo:hi]
+        xs = torch.zeros_like(b)
+        check(lib().psx_pcg(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), _lib.PSX_FP64, ptr(bs), ptr(xs), 1e-12,
+                            0.0, 200000, prec, ptr(work1), work1.numel(), ptr(st), _stream()), "psx_pcg")
+        assert st.cpu().numpy()[5] == 0
+        assert rel_2(x[lo:hi].cpu().numpy(), xs[lo:hi].cpu().numpy()) < 1e-9, s
