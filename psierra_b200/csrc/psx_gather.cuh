@@ -411,6 +411,34 @@ __device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
   return v;
 }
 
+// Bounded wait, executed by a whole warp: lane j checks counter[first + j] >=
+// target(first + j) for j < count.  Returns false (and flags the status) if the wait
+// gives up; the caller then still proceeds, so every access stays in bounds and the
+// host reports the failure.
+template <typename Target>
+__device__ __forceinline__ bool wait_counters(const int32_t* cnt, int32_t first, int32_t count, Target target,
+                                              Status* st, int32_t max_spins) {
+  const int lane = threadIdx.x & 31;
+  for (int32_t base = 0; base < count; base += 32) {
+    const int32_t g = first + base + lane;
+    const bool mine = (base + lane) < count && g >= 0;
+    const int32_t want = mine ? target(g) : 0;
+    int spins = 0;
+    while (true) {
+      const bool ok = !mine || ld_acquire(cnt + g) >= want;
+      if (__all_sync(0xffffffffu, ok)) break;
+      // once any wait has given up, every later wait returns at once
+      if (++spins > max_spins || (ld_acquire(&st->flags) & 1)) {
+        if (lane == 0) atomicOr(&st->flags, 1);
+        return false;
+      }
+      if (spins > 64) __nanosleep(200);
+    }
+    if (spins && lane == 0) atomicAdd(&st->iters, spins);
+  }
+  return true;
+}
+
 // Bounded wait on a prefix, executed by a whole warp: returns once every granule
 // g <= need has reached target(g).  `done` is the warp's watermark (every granule
 // <= done is known complete; start at -1): a wait below it costs nothing, and each poll
@@ -464,7 +492,9 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
     return (int32_t)((n + Q.tile - 1) / Q.tile);
   };
   auto btiles = [&](int32_t r) -> int32_t { return __ldg(Q.btiles + r); };
-  int32_t evaluated = -1, gathered = -1;  // watermarks of wait_prefix
+  // this loop keeps the span waits: prefix waits (wait_prefix, as in the split kernel's
+  // loops) measured slower here, where one warp runs both kinds of task (K.v 0.298 ->
+  // 0.351 ms, f only 0.284 -> 0.350 ms on the 80^3 cube)
   int32_t next = 0;
   if (lane == 0) next = atomicAdd(Q.counters, 1);
   while (true) {
@@ -475,8 +505,7 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
     const int32_t gr = task.y;
     if (task.x == 0) {
       const int32_t old = gr - Q.ring_g;  // granule whose ring slots this tile overwrites
-      if (old >= 0)
-        wait_prefix(bcnt, min(old + Q.span_g + 1, Q.n_granules - 1), Q.n_granules, btiles, gathered, st, Q.max_spins);
+      if (old >= 0) wait_counters(bcnt, old, min(Q.span_g + 2, Q.n_granules - old), btiles, st, Q.max_spins);
       __syncwarp();
       element_tile(task);
       __syncwarp();
@@ -485,7 +514,8 @@ __device__ __forceinline__ void drain_queue(const GatherArgs& g, const QueueArgs
         atomicAdd(acnt + gr, 1);
       }
     } else {
-      wait_prefix(acnt, gr, Q.n_granules, atiles, evaluated, st, Q.max_spins);
+      const int32_t first = max(0, gr - Q.span_g - 1);
+      wait_counters(acnt, first, gr - first + 1, atiles, st, Q.max_spins);
       __syncwarp();
       for (int32_t item = task.z + lane; item < task.w; item += 32) {
         // K row segments leave as vector + scalar pairs (FP64 f+K 2.35 -> 2.26 ms, Tet10

@@ -565,6 +565,7 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
       const int a0 = off[lp], a1 = off[lp + 1];
       float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
       float s2 = 0.f;
+      #pragma unroll 1
       for (int q = a0; q < a1; ++q) {
         const int c = src[q];
         const float* b = kst + (c >> 3) * kStageStride + L::pair_off(c & 7);
@@ -589,6 +590,7 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
     float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f);
     float2 d1 = make_float2(0.f, 0.f);
     double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    #pragma unroll 1
     for (int q = a0; q < a1; ++q) {
       const int c = src[q];
       const int el = c >> 2, a = c & 3;

@@ -3,12 +3,12 @@
 The kernel's wait rules, restated:
 * gather tiles of granule r are queued after the element tiles of granule r + 1 + lag;
 * an element tile of granule g waits for all gather tiles of granules
-  [0, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
+  [g - R, g - R + span_g + 1] (R = ring length in granules) before overwriting the ring
   slots of granule g - R, if g - R >= 0;
-* a gather tile of granule r waits for all element tiles of granules [0, r].
-Both waits are on prefixes (each warp keeps a watermark of the granules it knows are
-complete); the spans the ring needs, [g - R, g - R + span_g + 1] and [r - span_g - 1, r],
-are inside them.
+* a gather tile of granule r waits for all element tiles of granules [r - span_g - 1, r].
+The warp-specialised kernel's loops wait on prefixes instead ([0, g - R + span_g + 1] and
+[0, r]: each warp keeps a watermark of the granules it knows are complete), which contain
+those spans.
 Tasks are claimed in queue order by running blocks, so the queue always drains if every
 task only waits on tasks strictly earlier in the queue.  Ring safety: every gather item
 that reads an element of granule q belongs to a granule in [q, q + span_g + 1].
@@ -77,10 +77,10 @@ def test_waits_only_on_earlier_tasks(granule, with_pairs, lag):
         if kind == 0:
             old = g - ring
             if old >= 0:
-                for r in range(0, min(old + span_g + 2, G)):
+                for r in range(old, min(old + span_g + 2, G)):
                     assert last_b.get(r, -1) < q, "element tile waits on a later gather tile"
         else:
-            for gp in range(0, g + 1):
+            for gp in range(max(0, g - span_g - 1), g + 1):
                 assert last_a[gp] < q, "gather tile waits on a later element tile"
     # ring safety: items read elements within span_g + 1 granules of their own granule
     for kind, g, b, e in tasks[kinds != 0]:
