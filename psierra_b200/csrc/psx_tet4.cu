@@ -929,11 +929,13 @@ extern "C" int psx_tet4_assemble_effective(const psx_plan_t* plan, const double*
              c_t, c_m, c_0, rho};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   constexpr int kFK = PSX_WANT_F | PSX_WANT_K | kModeEff, kK = PSX_WANT_K | kModeEff;
+  // the FP32 effective tangent takes the warp-specialised kernel like K_T itself (the
+  // element math is explicitly rounded, so both kernels give the same bits)
   if (mode & PSX_WANT_F)
     return precision == PSX_FP64 ? run_tet4<double, kFK>(plan, A, W, static_cast<double*>(k_out), f_out, s)
-                                 : run_tet4<float, kFK>(plan, A, W, static_cast<float*>(k_out), f_out, s);
+                                 : run_tet4_k32<kFK>(plan, A, W, static_cast<float*>(k_out), f_out, s);
   return precision == PSX_FP64 ? run_tet4<double, kK>(plan, A, W, static_cast<double*>(k_out), nullptr, s)
-                               : run_tet4<float, kK>(plan, A, W, static_cast<float*>(k_out), nullptr, s);
+                               : run_tet4_k32<kK>(plan, A, W, static_cast<float*>(k_out), nullptr, s);
 }
 
 extern "C" int psx_tet4_kv(const psx_plan_t* plan, const double* X, const double* u, const double* mu_e,

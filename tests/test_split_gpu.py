@@ -60,3 +60,25 @@ def test_split_kernel_equals_mixed_kernel_bitwise(name):
     # repeated calls reuse the counters and the ring: still the same bits
     f2, k2 = a.assemble(u)
     assert torch.equal(f2, out[True][0]) and torch.equal(k2, out[True][1])
+
+
+@pytest.mark.parametrize("name", ["ragged box", "cube 40"])
+def test_effective_tangent_split_equals_mixed_kernel_bitwise(name):
+    """c_t K_T + c_m M + c_0 K_0 (the dynamic effective tangent) through the
+    warp-specialised kernel gives the mixed kernel's bits."""
+    mesh = MESHES[name]()
+    E = mesh.n_elements
+    mu = np.random.default_rng(5).uniform(1e3, 5e3, E)
+    a = GPUAssembler(mesh.nodes, mesh.elements, NeoHookeanField(mu, 20.0 * mu, mass_density=1000.0),
+                     precision="fp32-mixed")
+    X = mesh.nodes
+    uf = 0.02 * (X[:, [2, 0, 1]] - X.mean(axis=0))
+    u = torch.from_numpy(np.ascontiguousarray(uf).reshape(-1)).to(DEV)
+    out = {}
+    for split in (False, True):
+        a.set_queue(split=split)
+        f, k = a.assemble_effective(u, 0.9, 37.0, 0.0)
+        _, kk = a.assemble_effective(u, 0.9, 37.0, 0.0, want_f=False)
+        out[split] = (f.clone(), k.clone(), kk.clone())
+    for x, y in zip(out[False], out[True]):
+        assert torch.equal(x, y), name
