@@ -37,6 +37,8 @@ class DeviceNewtonResult:
 class DeviceNewton:
     def __init__(self, asm: GPUAssembler, fixed_dofs, precision: str | None = None, pcg_tol: float = 1e-10,
                  pcg_maxiter: int = 20000, preconditioner: str = "block-jacobi") -> None:
+        """``preconditioner``: "jacobi", "block-jacobi" or "two-level" (block-Jacobi plus
+        the rigid-body modes of slices of the mesh, ``psierra_b200.coarse``)."""
         self.asm = asm
         self.precision = precision or asm.precision
         dev = asm.device
@@ -46,6 +48,12 @@ class DeviceNewton:
         mask[np.asarray(fixed_dofs, dtype=np.int64)] = 1
         self.fixed = torch.from_numpy(mask).to(dev)
         self.free = torch.from_numpy(mask == 0).to(dev)
+        self.coarse = None
+        if preconditioner == "two-level":
+            from psierra_b200.coarse import CoarseSpace
+
+            self.coarse = CoarseSpace(asm.X.view(-1, 3).cpu().numpy(), asm.pattern.conn, mask, device=dev)
+            preconditioner = "block-jacobi"
         self.pcg = ConjugateGradientSolver(tolerance=pcg_tol, max_iterations=pcg_maxiter,
                                            preconditioner=preconditioner, device=dev)
         self.f = asm.new_f()
@@ -68,7 +76,9 @@ class DeviceNewton:
         """K x = rhs with the current eliminated tangent; rhs must be zero on fixed DOFs."""
         d = self.asm.dev
         x = torch.zeros_like(rhs)
-        res = self.pcg.solve_device(d["indptr"], d["indices"], self.k, rhs, x, nodal=True)
+        if self.coarse is not None:
+            self.coarse.update(self.k, d["indptr"], d["indices"])
+        res = self.pcg.solve_device(d["indptr"], d["indices"], self.k, rhs, x, nodal=True, coarse=self.coarse)
         if not res.converged:
             raise RuntimeError(f"Conjugate Gradient did not converge (info={res.iterations}).")
         return x, res.iterations

@@ -100,11 +100,13 @@ class ConjugateGradientSolver(SparseLinearSolver):
         return self._work
 
     def solve_device(self, indptr: torch.Tensor, indices: torch.Tensor, values: torch.Tensor, b: torch.Tensor,
-                     x: torch.Tensor, nodal: bool = False) -> PCGResult:
+                     x: torch.Tensor, nodal: bool = False, coarse=None) -> PCGResult:
         """Solve in place on device tensors (``x`` holds the initial guess on entry).
 
         ``nodal``: the CSR is node-blocked (``is_nodal_csr``; every matrix of the
         assembler's pattern is), so the SpMVs read each neighbour's columns once per node.
+        ``coarse``: a ``psierra_b200.coarse.CoarseSpace`` already updated from ``values``;
+        its rigid-body-mode correction is added to the block-Jacobi preconditioner.
         """
         n = b.numel()
         precond = PRECONDITIONERS[self.preconditioner]
@@ -120,9 +122,17 @@ class ConjugateGradientSolver(SparseLinearSolver):
         if self._status is None:
             self._status = torch.zeros(8, dtype=torch.int32, device=self.device)
         work = self._workspace(n, precond)
-        check(lib().psx_pcg(n, ptr(indptr), ptr(indices), ptr(values), vp, ptr(b), ptr(x), float(self.tolerance),
-                            float(self.atol), int(self.max_iterations), precond, ptr(work), work.numel(),
-                            ptr(self._status), torch.cuda.current_stream().cuda_stream), "psx_pcg")
+        if coarse is not None:
+            if (precond & ~_lib.PSX_PCG_NODAL) != _lib.PSX_PRECOND_BJACOBI:
+                raise ValueError("the coarse correction is added to the block-jacobi preconditioner")
+            check(lib().psx_pcg_coarse(n, ptr(indptr), ptr(indices), ptr(values), vp, ptr(b), ptr(x),
+                                       float(self.tolerance), float(self.atol), int(self.max_iterations), precond,
+                                       coarse.struct_ptr(), ptr(work), work.numel(), ptr(self._status),
+                                       torch.cuda.current_stream().cuda_stream, 1), "psx_pcg_coarse")
+        else:
+            check(lib().psx_pcg(n, ptr(indptr), ptr(indices), ptr(values), vp, ptr(b), ptr(x), float(self.tolerance),
+                                float(self.atol), int(self.max_iterations), precond, ptr(work), work.numel(),
+                                ptr(self._status), torch.cuda.current_stream().cuda_stream), "psx_pcg")
         st = self._status.cpu()
         iters, flags = int(st[4]), int(st[5])
         rn = float(st.view(torch.float64)[3])

@@ -137,19 +137,22 @@ def test_batched_newton_two_level_matches_block_jacobi():
         assert rel_2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6
 
 
-@pytest.mark.parametrize("coarse", [False, True])
-def test_batched_cg_solves_each_instance_like_its_own_cg(coarse):
+@pytest.mark.parametrize("coarse,precision,nodal", [(False, "fp64", True), (True, "fp64", True),
+                                                    (True, "fp32-mixed", True), (True, "fp64", False)])
+def test_batched_cg_solves_each_instance_like_its_own_cg(coarse, precision, nodal):
     """psx_pcg_batched: one CG per segment of a block-diagonal system; each segment's
     solution equals that instance's own solve (psx_pcg, block-Jacobi) to the solver
-    tolerance, and the segments converge with their own iteration counts."""
-    meshes, union, node_off, asm, fixed = _two_beams()
-    k = _eliminated_tangent(asm, fixed, "fp64")
+    tolerance, and the segments converge with their own iteration counts (FP64 or FP32
+    matrix values, node-blocked or row-wise SpMV)."""
+    meshes, union, node_off, asm, fixed = _two_beams(precision)
+    k = _eliminated_tangent(asm, fixed, precision)
+    vp = _lib.PSX_FP64 if k.dtype == torch.float64 else _lib.PSX_FP32_MIXED
     d = asm.dev
     n = 3 * union.n_nodes
     f = np.concatenate([meshgen.traction_nodal_forces(m, int(np.argmax(np.ptp(m.nodes, axis=0))), "max",
                                                       [0.0, 0.0, -10.0 * (1 + 99 * b)]) for b, m in enumerate(meshes)])
     b = torch.from_numpy(f * (fixed == 0)).to(DEV)
-    prec = _lib.PSX_PRECOND_BJACOBI | _lib.PSX_PCG_NODAL
+    prec = _lib.PSX_PRECOND_BJACOBI | (_lib.PSX_PCG_NODAL if nodal else 0)
     B = len(meshes)
     seg_off = torch.from_numpy(3 * np.asarray(node_off, dtype=np.int64)).to(DEV)
     node_seg = torch.from_numpy(np.repeat(np.arange(B, dtype=np.int32), np.diff(node_off))).to(DEV)
@@ -163,7 +166,7 @@ def test_batched_cg_solves_each_instance_like_its_own_cg(coarse):
     st = torch.zeros((int(lib().psx_status_bytes()) + 3) // 4, dtype=torch.int32, device=DEV)
     seg_iters = torch.zeros(B, dtype=torch.int32, device=DEV)
     x = torch.zeros(n, dtype=torch.float64, device=DEV)
-    check(lib().psx_pcg_batched(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), _lib.PSX_FP64, ptr(b), ptr(x), 1e-12,
+    check(lib().psx_pcg_batched(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), vp, ptr(b), ptr(x), 1e-12,
                                 0.0, 20000, prec, B, ptr(seg_off), ptr(node_seg),
                                 cs.struct_ptr() if cs is not None else None, ptr(work), work.numel(), ptr(st),
                                 ptr(seg_iters), _stream()), "psx_pcg_batched")
@@ -177,7 +180,29 @@ def test_batched_cg_solves_each_instance_like_its_own_cg(coarse):
         lo, hi = 3 * int(node_off[s]), 3 * int(node_off[s + 1])
         bs[lo:hi] = b[lo:hi]
         xs = torch.zeros_like(b)
-        check(lib().psx_pcg(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), _lib.PSX_FP64, ptr(bs), ptr(xs), 1e-12,
+        check(lib().psx_pcg(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(k), vp, ptr(bs), ptr(xs), 1e-12,
                             0.0, 200000, prec, ptr(work1), work1.numel(), ptr(st), _stream()), "psx_pcg")
         assert st.cpu().numpy()[5] == 0
         assert rel_2(x[lo:hi].cpu().numpy(), xs[lo:hi].cpu().numpy()) < 1e-9, s
+
+
+def test_device_newton_two_level_matches_block_jacobi():
+    """DeviceNewton with the two-level preconditioner on a slender clamped beam: the same
+    Newton iterations and displacement as block-Jacobi, in far fewer CG iterations."""
+    from psierra_b200.newton import DeviceNewton
+
+    m = meshgen.box_tet4(1.5, 0.1, 0.1, 60, 4, 4)
+    mu, _, kappa = meshgen.lame_from_young_poisson(1e5, 0.3)
+    f = torch.from_numpy(meshgen.traction_nodal_forces(m, 0, "max", [20.0, 0.0, -2.0])).to(DEV)
+    clamp = meshgen.nodes_on_plane(m, 0, "min")
+    fixed = np.concatenate([3 * clamp + c for c in range(3)])
+    out = {}
+    for pre in ("block-jacobi", "two-level"):
+        asm = GPUAssembler(m.nodes, m.elements, NeoHookeanField(np.full(m.n_elements, mu), np.full(m.n_elements, kappa)))
+        nt = DeviceNewton(asm, fixed, precision="fp64", pcg_tol=1e-12, pcg_maxiter=100000, preconditioner=pre)
+        res = nt.solve(f, n_steps=2, nr_iterations=20, nr_tol=1e-10)
+        assert res.converged, pre
+        out[pre] = (res.u.cpu().numpy(), res.iteration_history, sum(res.pcg_iterations))
+    assert out["two-level"][1] == out["block-jacobi"][1]
+    assert rel_2(out["two-level"][0], out["block-jacobi"][0]) < 1e-9
+    assert out["two-level"][2] * 4 < out["block-jacobi"][2], (out["two-level"][2], out["block-jacobi"][2])
