@@ -206,3 +206,40 @@ def test_device_newton_two_level_matches_block_jacobi():
     assert out["two-level"][1] == out["block-jacobi"][1]
     assert rel_2(out["two-level"][0], out["block-jacobi"][0]) < 1e-9
     assert out["two-level"][2] * 4 < out["block-jacobi"][2], (out["two-level"][2], out["block-jacobi"][2])
+
+
+def test_batched_cg_isolates_a_non_finite_instance():
+    """A retired instance whose tangent block holds NaN (its displacement inverted
+    elements) gets a zero right-hand side; the other instances' CGs, which share the
+    launches but not the step lengths, must be unaffected: their solutions equal a solve
+    with finite values everywhere, bit for bit."""
+    meshes, union, node_off, asm, fixed = _two_beams()
+    k = _eliminated_tangent(asm, fixed, "fp64")
+    d = asm.dev
+    n = 3 * union.n_nodes
+    f = np.concatenate([meshgen.traction_nodal_forces(m, int(np.argmax(np.ptp(m.nodes, axis=0))), "max",
+                                                      [0.0, 0.0, -10.0]) for m in meshes])
+    b = torch.from_numpy(f * (fixed == 0)).to(DEV)
+    lo0, hi0 = 0, 3 * int(node_off[1])
+    b[lo0:hi0] = 0.0  # instance 0 retired
+    prec = _lib.PSX_PRECOND_BJACOBI | _lib.PSX_PCG_NODAL
+    B = len(meshes)
+    seg_off = torch.from_numpy(3 * np.asarray(node_off, dtype=np.int64)).to(DEV)
+    node_seg = torch.from_numpy(np.repeat(np.arange(B, dtype=np.int32), np.diff(node_off))).to(DEV)
+    nb = ctypes.c_int64()
+    check(lib().psx_pcg_batched_work_bytes(n, B, ctypes.byref(nb)), "psx_pcg_batched_work_bytes")
+    work = torch.empty(int(nb.value), dtype=torch.uint8, device=DEV)
+    st = torch.zeros((int(lib().psx_status_bytes()) + 3) // 4, dtype=torch.int32, device=DEV)
+    indptr = d["indptr"].cpu().numpy()
+    out = []
+    for poison in (False, True):
+        kk = k.clone()
+        if poison:  # every value in the rows of instance 0
+            kk[int(indptr[lo0]):int(indptr[hi0])] = float("nan")
+        x = torch.zeros(n, dtype=torch.float64, device=DEV)
+        check(lib().psx_pcg_batched(n, ptr(d["indptr"]), ptr(d["indices"]), ptr(kk), _lib.PSX_FP64, ptr(b), ptr(x),
+                                    1e-10, 0.0, 5000, prec, B, ptr(seg_off), ptr(node_seg), None, ptr(work),
+                                    work.numel(), ptr(st), None, _stream()), "psx_pcg_batched")
+        out.append(x.clone())
+    assert torch.equal(out[0][hi0:], out[1][hi0:])
+    assert torch.isfinite(out[1][hi0:]).all() and out[1][hi0:].abs().max() > 0
