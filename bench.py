@@ -41,7 +41,7 @@ WORKLOAD = ("cube 80^3 Kuhn Tet4 (3,072,000 elements, 531,441 nodes), NeoHookean
 # capture of the FP32-mixed f+K and K.v launches on the cube 56^3 (1,053,696 elements);
 # the traffic grows with the element count, so it is scaled by E for this workload.
 NCU_CAPTURE_ELEMENTS = 1053696
-NCU_TRAFFIC = {"fk32": 99.470592e6 + 125.007616e6, "kv32": 60.488704e6 + 2.76224e6}
+NCU_TRAFFIC = {"fk32": 98.47552e6 + 102.580736e6, "kv32": 52.138752e6 + 1.884416e6}
 
 
 def parse():
@@ -641,7 +641,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": NCU_TRAFFIC["fk32"] * E / NCU_CAPTURE_ELEMENTS,
                          "traffic_note": "bytes per launch: ncu DRAM read+write of the cube 56^3 launch scaled by "
-                                         "elements (latency-bound: DRAM throughput 11.3% in that capture of the split kernel)",
+                                         "elements (latency-bound: DRAM throughput 10.7% in that capture of the split kernel)",
                          "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": bytes_mixed, "kernel": fk_kernel,
                          "launches_per_step": asm.launches_per_call("fp32-mixed")},
