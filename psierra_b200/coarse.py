@@ -28,9 +28,12 @@ inverse as a matrix-vector product (``psx_pcg_coarse``).
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
+from psierra_b200 import _lib
 from psierra_b200._lib import CoarseStruct, check, lib, ptr
 
 
@@ -193,14 +196,11 @@ class CoarseSpace:
         return out
 
     def struct_ptr(self):
-        import ctypes
-
+        """``psx_coarse_t*`` for the C ABI."""
         return ctypes.byref(self.struct)
 
     def update(self, k: torch.Tensor, indptr: torch.Tensor, indices: torch.Tensor) -> None:
         """A_c = P^T K P by probing, then A_c^-1 per block, all on the current stream."""
-        from psierra_b200 import _lib
-
         vp = _lib.PSX_FP64 if k.dtype == torch.float64 else _lib.PSX_FP32_MIXED
         stream = torch.cuda.current_stream().cuda_stream
         n = 3 * self.n_nodes
