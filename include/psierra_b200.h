@@ -439,7 +439,8 @@ typedef struct psx_coarse_t {
   const uint8_t* fixed;      /* 3N: nonzero on eliminated unknowns */
   int32_t n_blocks;          /* independent coarse blocks */
   int32_t nc;                /* padded coarse size: >= 6 x the aggregates of any block */
-  const int32_t* block_agg;  /* n_blocks + 1: block b holds aggregates [block_agg[b], block_agg[b+1]) */
+  const int32_t* block_agg;  /* n_blocks + 1: block b holds aggregates [block_agg[b], block_agg[b+1]); a block with
+                                6 x its aggregates > nc gets no coarse correction */
   const double* ainv;        /* n_blocks x nc x nc, row-major: A_c^-1 of each block (6 (a - block_agg[b]) + t) */
   double* rc;                /* 6 n_agg scratch */
   double* yc;                /* 6 n_agg scratch */

@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(kBlock) coarse_gemv_kernel(psx_coarse_t c, con
   extern __shared__ double s_rhs[];
   const int32_t a0 = c.block_agg[blockIdx.x];
   const int m = 6 * (c.block_agg[blockIdx.x + 1] - a0);
+  if (m < 0 || m > c.nc) return;  // inconsistent block sizes: stay inside the staged right-hand side
   for (int k = threadIdx.x; k < m; k += kBlock) s_rhs[k] = c.rc[6 * (int64_t)a0 + k];
   __syncthreads();
   const double* A = c.ainv + (int64_t)blockIdx.x * c.nc * c.nc;
