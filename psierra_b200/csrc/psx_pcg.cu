@@ -28,7 +28,11 @@ namespace psx {
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kGridMax = 148 * 4;
+// Five blocks per SM: the node-blocked SpMV (48 registers) fits five, and the PCG
+// iteration on the 3.07M-element cube takes 0.153 ms instead of 0.157 with four; six
+// (launch bounds capping 40 registers) measured 0.169 ms; prefetching the next node's
+// row range one pass ahead, 0.157 ms.
+constexpr int kGridMax = 148 * 5;
 constexpr int kRowLanes = 8;  // lanes per CSR row in the SpMV
 
 struct PcgScalars {
@@ -188,6 +192,7 @@ __device__ __forceinline__ double spmv_row(int64_t n, int64_t row, int lane8, co
 // Scalar loads: the 8 lanes of a group read 24 consecutive values of a row per load
 // instruction.  Loading each row segment and x triple as an aligned pair plus a scalar
 // (9 instead of 13 loads per neighbour) measured slower: 0.194 instead of 0.155 ms.
+// Unrolling the neighbour loop by 2 or 4 did too: 0.171 and 0.158 instead of 0.156 ms.
 constexpr int kNodeLanes = 8;  // PCG iteration on the 3.07M-element cube: 0.157 ms (16 lanes 0.176, 4 lanes 0.165)
 template <typename VT>
 __device__ __forceinline__ void spmv_node(int64_t nodes, int64_t node, int lane16, const int32_t* __restrict__ indptr,
