@@ -154,7 +154,12 @@ class _GPUElementBase:
         if u.size != self._u_dev.numel():
             raise ValueError(f"displacement has {u.size} entries, expected {self._u_dev.numel()}")
         pin = self._staging.get("u", u.size, torch.float64)
-        pin.numpy()[:] = u
+        # torch's copy runs on all host threads (12.8 MB of the 80^3 cube: 0.3 ms instead
+        # of the 1.6 ms of a numpy assignment); a read-only array takes the numpy route
+        if u.flags.writeable:
+            pin.copy_(torch.from_numpy(u))
+        else:
+            pin.numpy()[:] = u
         self._u_dev.copy_(pin, non_blocking=True)
         return self._u_dev
 
