@@ -97,11 +97,11 @@ __device__ __forceinline__ void store_block(KT* __restrict__ p, const KT v[N]) {
   } else if constexpr (sizeof(KT) == 4) {
     float4* q = reinterpret_cast<float4*>(p);
 #pragma unroll
-    for (int i = 0; i < N / 4; ++i) __stcg(q + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+    for (int i = 0; i < N / 4; ++i) st_ring(q + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
   } else {
     double2* q = reinterpret_cast<double2*>(p);
 #pragma unroll
-    for (int i = 0; i < N / 2; ++i) __stcg(q + i, make_double2(v[2 * i], v[2 * i + 1]));
+    for (int i = 0; i < N / 2; ++i) st_ring(q + i, make_double2(v[2 * i], v[2 * i + 1]));
   }
 }
 
@@ -117,9 +117,9 @@ __device__ __forceinline__ void store_planes(KT* __restrict__ base, int o, const
   for (int i = 0; i < N / W; ++i) {
     KT* q = base + (int64_t)(o / W + i) * plane * W;
     if constexpr (W == 4)
-      __stcg(reinterpret_cast<float4*>(q), make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+      st_ring(reinterpret_cast<float4*>(q), make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
     else
-      __stcg(reinterpret_cast<double2*>(q), make_double2(v[2 * i], v[2 * i + 1]));
+      st_ring(reinterpret_cast<double2*>(q), make_double2(v[2 * i], v[2 * i + 1]));
   }
 }
 template <typename KT, int N>

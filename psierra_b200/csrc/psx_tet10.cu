@@ -238,9 +238,9 @@ __device__ __forceinline__ void tet10_tile(const Tet10Args& A, const int4& task,
       }
       if (active && q == 0) {
         double* fr = frec + (e & ring_mask) * L10::kF + 3 * a;
-        __stcg(fr, fa[0]);
-        __stcg(fr + 1, fa[1]);
-        __stcg(fr + 2, fa[2]);
+        st_ring(fr, fa[0]);
+        st_ring(fr + 1, fa[1]);
+        st_ring(fr + 2, fa[2]);
       }
     }
     if constexpr (kWantK) {

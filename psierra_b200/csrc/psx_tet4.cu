@@ -574,9 +574,9 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
         s1.x += y.x; s1.y += y.y; s1.z += y.z; s1.w += y.w;
         s2 += b[8];
       }
-      __stcg(p0 + lp, s0);
-      __stcg(p1 + lp, s1);
-      __stcg(p2 + lp, s2);
+      st_ring(p0 + lp, s0);
+      st_ring(p1 + lp, s1);
+      st_ring(p2 + lp, s2);
     }
   }
   const int nn = lst[1];
@@ -609,13 +609,13 @@ __device__ __forceinline__ void tile_reduce(const GatherArgs& g, int64_t t, cons
       }
     }
     if constexpr (WANT_K) {
-      __stcg(d0p + ln, d0);
-      __stcg(d1p + ln, d1);
+      st_ring(d0p + ln, d0);
+      st_ring(d1p + ln, d1);
     }
     if constexpr (WANT_F) {
-      __stcg(fb + ln, f0);
-      __stcg(fb + g.cap_n4 + ln, f1);
-      __stcg(fb + 2 * g.cap_n4 + ln, f2);
+      st_ring(fb + ln, f0);
+      st_ring(fb + g.cap_n4 + ln, f1);
+      st_ring(fb + 2 * g.cap_n4 + ln, f2);
     }
   }
 }
