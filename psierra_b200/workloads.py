@@ -10,6 +10,8 @@ seeded synthetic meshes and fields (the reference's own meshes are not used).
   -0.2 prescribed and ramped over 20 increments; every Newton step solved by Jacobi PCG
   to rtol 1e-8 (psierra ``analysis/nonlinear_static.py:250-404``,
   ``solver/sparse_linear_solver.py:37-68``).  FP64 and FP32-mixed tangents.
+  ``--preconditioner block-jacobi|two-level`` swaps the PCG's preconditioner (same
+  tolerance, so the same answer to within it).
 * cfg4 -- adjoint identification on the ellipsoid (80 x 60 x 70 mm, 2 mm Kuhn grid
   clipped to the ellipsoid: every corner inside), per-element mu ~ LogNormal(ln 1000 Pa,
   0.3), kappa = 50 mu, density 1040, gravity through the consistent mass (a stated
@@ -41,7 +43,7 @@ def _nh(E, nu, rho=1000.0):
 
 
 def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), pcg_rtol: float = 1e-8,
-         nr_iterations: int = 30) -> dict:
+         nr_iterations: int = 30, preconditioner: str = "jacobi") -> dict:
     m = meshgen.tet4_to_tet10(meshgen.box_tet4(1.0, 1.0, 1.0, cells, cells, cells))
     bottom = meshgen.nodes_on_plane(m, 2, "min")
     top = meshgen.nodes_on_plane(m, 2, "max")
@@ -51,13 +53,16 @@ def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), 
     up[torch.from_numpy(3 * top + 2).to(dev)] = -0.2
     f_ext = torch.zeros(m.n_dofs, dtype=torch.float64, device=dev)
     out = {"workload": f"cfg3: cube {cells}^3 Kuhn -> {m.n_elements} Tet10, {m.n_nodes} nodes ({m.n_dofs} DOFs), "
-                       f"E=1e4 nu=0.4, top u_z=-0.2 over {n_steps} increments, Jacobi PCG rtol {pcg_rtol}, "
+                       f"E=1e4 nu=0.4, top u_z=-0.2 over {n_steps} increments, {preconditioner} PCG rtol {pcg_rtol}, "
                        f"at most {nr_iterations} Newton iterations per increment"}
     us = {}
     for prec in precisions:
         asm = GPUAssembler(m.nodes, m.elements, _nh(1e4, 0.4), precision=prec)
-        nt = DeviceNewton(asm, fixed, precision=prec, pcg_tol=pcg_rtol, pcg_maxiter=100000, preconditioner="jacobi")
+        t_setup = time.perf_counter()
+        nt = DeviceNewton(asm, fixed, precision=prec, pcg_tol=pcg_rtol, pcg_maxiter=100000,
+                          preconditioner=preconditioner)
         torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t_setup
         t0 = time.perf_counter()
         res = nt.solve(f_ext, u_prescribed=up, n_steps=n_steps, nr_iterations=nr_iterations, nr_tol=1e-8)
         torch.cuda.synchronize()
@@ -65,6 +70,7 @@ def cfg3(cells: int = 30, n_steps: int = 20, precisions=("fp64", "fp32-mixed"), 
         us[prec] = res.u
         out[prec.replace("-", "_")] = {
             "converged": bool(res.converged), "steps": res.steps_completed, "seconds": dt,
+            "solver_setup_seconds": t_setup,
             "newton_iterations": int(sum(res.iteration_history)), "newton_per_step": res.iteration_history,
             "pcg_iterations": int(sum(res.pcg_iterations)),
             "final_relative_residual": (res.residual_history[-1] / max(res.residual_history[0], 1e-300)
@@ -193,16 +199,18 @@ def main(argv=None) -> None:
     ap.add_argument("--fd-elements", type=int, default=32, help="cfg4: elements checked by central differences")
     ap.add_argument("--fd-step", type=float, default=1e-6, help="cfg4: central-difference step / mu_e")
     ap.add_argument("--beams", type=int, default=256, help="cfg5: instances")
-    ap.add_argument("--preconditioner", default="two-level", help="cfg5: block-jacobi or two-level")
+    ap.add_argument("--preconditioner", default=None,
+                    help="cfg3 (default jacobi, as configured) and cfg5 (default two-level): jacobi, block-jacobi "
+                         "or two-level")
     ap.add_argument("--pcg-iterations", type=int, default=None, help="cfg5: CG iterations per Newton step")
     a = ap.parse_args(argv)
     if a.workload == "cfg3":
         rec = cfg3(cells=a.cells, n_steps=a.steps, precisions=tuple(a.precisions.split(",")), pcg_rtol=a.pcg_rtol,
-                   nr_iterations=a.nr_iterations)
+                   nr_iterations=a.nr_iterations, preconditioner=a.preconditioner or "jacobi")
     elif a.workload == "cfg4":
         rec = cfg4(h_grid=a.grid, gravity_fraction=a.gravity, n_check=a.fd_elements, rel_step=a.fd_step)
     else:
-        rec = cfg5(n=a.beams, target_tets=4.1e6 * a.beams / 256, preconditioner=a.preconditioner,
+        rec = cfg5(n=a.beams, target_tets=4.1e6 * a.beams / 256, preconditioner=a.preconditioner or "two-level",
                    pcg_iterations=a.pcg_iterations)
     print(json.dumps(rec))
 
