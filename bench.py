@@ -33,7 +33,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Tet4 f_int+K_T elems/s and K·v HBM GB/s, FP32-mixed vs FP64 at ≤1e-6 rel"
-WORKLOAD = ("cube 80^3 Kuhn Tet4 (3,072,000 elements, 531,441 nodes), NeoHookean E=3e3 nu=0.45, "
+def workload(cells: int, elements: int, nodes: int) -> str:
+    """The workload line of ``config``: the cube of ``cells``^3 Kuhn cells (80 by default)."""
+    return (f"cube {cells}^3 Kuhn Tet4 ({elements:,} elements, {nodes:,} nodes), NeoHookean E=3e3 nu=0.45, "
             "u=0.05 sin(pi x) sin(pi y) z e_z + U(+-1e-4); one fused f_int+K_T assembly per step")
 
 
@@ -238,7 +240,7 @@ def time_steps_flushed(fn, steps: int, warmup: int, sync_all, flush):
     return sum(a.elapsed_time(b) for a, b in ev) / steps
 
 
-def dr_benchmark(asm, k_vals, u_dev, m, iterations: int, sync_all):
+def dr_benchmark(asm, k_vals, u_dev, m, iterations: int, sync_all, cells: int = 80):
     """The workload's dynamic relaxation: ``iterations`` fused matrix-free pseudo-steps
     (K_T(u) x on the fly, the viscous update of psierra analysis/dynamic_relaxation.py:
     296-299, 378-382 with damping c = 0.1, dt = 1), per precision, on the cube clamped at
@@ -266,7 +268,7 @@ def dr_benchmark(asm, k_vals, u_dev, m, iterations: int, sync_all):
     E, N = m.n_elements, m.n_nodes
     # conn, X, u; x read, b, 1/m, vel read + write, x write
     bytes_it = 16 * E + 48 * N + 24 * N * 6
-    out = {"workload": "cube 80^3 clamped at z = 0, Gerschgorin lumped mass (sf 1.1), damping 0.1, dt 1; "
+    out = {"workload": f"cube {cells}^3 clamped at z = 0, Gerschgorin lumped mass (sf 1.1), damping 0.1, dt 1; "
                        f"{iterations} fused K(u)-matrix-free pseudo-steps (psx_tet4_dr_step) per precision",
            "iterations": iterations, "algorithmic_bytes_per_iteration": bytes_it}
     for prec in ("fp32-mixed", "fp64"):
@@ -371,7 +373,8 @@ def main():
             "impl": "reference", "metric": METRIC, "value": v, "unit": "elements/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * m.n_elements / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "elements": m.n_elements, "nodes": m.n_nodes},
+            "config": {"workload": workload(args.cells, m.n_elements, m.n_nodes), "elements": m.n_elements,
+                       "nodes": m.n_nodes},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}))
         return
@@ -449,7 +452,7 @@ def main():
 
     dr = None
     if args.dr_iterations > 0:
-        dr = dr_benchmark(asm, k32, u_dev, m, args.dr_iterations, sync_all)
+        dr = dr_benchmark(asm, k32, u_dev, m, args.dr_iterations, sync_all, cells=args.cells)
 
     if world > 1:
         t = torch.tensor([ms_mixed, ms_fp64], device=dev)
@@ -634,9 +637,10 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32-mixed (K_T f32; f_int, det F, ln J f64)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "elements": E, "nodes": N, "nnz": nnz,
-                       "l2": "assembly: working set exceeds L2 (K values 281 MB fp32 / 563 MB fp64 vs 126 MB L2); "
-                             "K.v: 512 MB L2 flush before every timed step",
+            "config": {"workload": workload(args.cells, E, N), "elements": E, "nodes": N, "nnz": nnz,
+                       "l2": (f"assembly: working set {'exceeds' if 4 * nnz > 126e6 else 'within'} L2 (K values "
+                              f"{4 * nnz / 1e6:.0f} MB fp32 / {8 * nnz / 1e6:.0f} MB fp64 vs 126 MB L2); "
+                              "K.v: 512 MB L2 flush before every timed step"),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": NCU_TRAFFIC["fk32"] * E / NCU_CAPTURE_ELEMENTS,

@@ -1,0 +1,33 @@
+"""The benchmark's reference arm on the host (CPU): ``bench.py --impl reference`` prints one
+JSON line with the keys of the benchmark contract, timing the oracle port of the
+reference's element sweeps and COO->CSR on the host cores for the same workload."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "0", "--cells", "5"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["unit"] == "elements/s" and d["value"] > 0 and d["higher_is_better"] is True
+    assert (d["n_gpus"], d["steps"], d["warmup"]) == (1, 2, 0)
+    assert d["vs_baseline"] is None and d["data"] == "synthetic"
+    assert d["config"]["elements"] == 6 * 5 ** 3 and d["config"]["nodes"] == 6 ** 3
+    assert d["config"]["workload"].startswith("cube 5^3 Kuhn Tet4 (750 elements, 216 nodes)")
+    assert abs(d["ms_per_step"] - 1e3 * d["config"]["elements"] / d["value"]) < 1e-6 * d["ms_per_step"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
