@@ -92,6 +92,49 @@ def element_fixture(rng, n, npe):
     return dict(X=X, u=u, E=E, nu=nu, mu=mu, kappa=kap, lam=lam, k=k, f=f, k_lin=klin)
 
 
+def element_extreme_fixture(npe: int = 4, n: int = 40, seed: int = 8):
+    """Elements far from element_fixture's states, through the reference's element:
+    homogeneous stretch and compression with rotation (det F from 0.35 to 2.5) plus a
+    non-homogeneous part, Poisson ratios up to 0.4999, and strains of 1e-7, where the
+    reference's stress formula carries its O(mu) cancellation.  Its own random stream,
+    so it can be regenerated alone."""
+    rng = np.random.default_rng(seed + npe)
+    nus = (0.3, 0.45, 0.49, 0.499, 0.4999)
+    dets = (0.35, 0.6, 1.8, 2.5)
+    keys = ("X", "u", "E", "nu", "mu", "kappa", "lam", "k", "f", "det_F")
+    rows = {k: [] for k in keys}
+    while len(rows["X"]) < n:
+        i = len(rows["X"])
+        X = random_tets(rng, 1, npe)[0]
+        scale = float(np.abs(X[1:4] - X[0]).max())
+        if i % 4 == 3:
+            u = rng.normal(0, 1, size=X.shape) * 1e-7 * scale
+            det_F = 1.0
+        else:
+            Rq, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            Qq, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            lam_p = np.exp(rng.normal(0, 0.35, size=3))
+            det_F = dets[(i // 4 + i) % len(dets)]
+            lam_p *= (det_F / lam_p.prod()) ** (1.0 / 3.0)
+            if np.linalg.det(Rq) * np.linalg.det(Qq) < 0:
+                Rq[:, 0] = -Rq[:, 0]  # proper rotations only: det F = det_F > 0
+            F = Rq @ np.diag(lam_p) @ Qq.T
+            c = X[:4].mean(axis=0)
+            u = (X - c) @ (F - np.identity(3)).T + rng.normal(0, 0.02 * scale, size=X.shape)
+        E = float(rng.uniform(1e3, 1e6))
+        nu = nus[i % len(nus)]
+        mat = nh(E, nu)
+        el = Tet4TotalLagrangian(mat) if npe == 4 else Tet10TotalLagrangian(mat)
+        try:
+            k, f = el.compute_nonlinear_force_and_tangent_stiffness(X, u)
+        except ValueError:
+            continue  # the perturbation inverted a quadrature point: draw again
+        for key, v in zip(keys, (X, u, E, nu, mat.parameters.shear_modulus, mat.parameters.bulk_modulus,
+                                 mat.parameters.lame_parameter_1, k, f, det_F)):
+            rows[key].append(v)
+    return {k: np.asarray(v) for k, v in rows.items()}
+
+
 def material_fixture(rng, n=24):
     Fs, Cs, Ss = [], [], []
     for _ in range(n):
@@ -238,7 +281,9 @@ def main(only=None):
         # fixtures that need no shared random stream can be regenerated on their own
         gens = {"fbar_box": fbar_fixture, "dynamic_beam": dynamic_fixture, "tet10_newton": tet10_newton_fixture,
                 "tet10_compress6": tet10_compress6_fixture,
-                "dynamic_tet10": dynamic_tet10_fixture}
+                "dynamic_tet10": dynamic_tet10_fixture,
+                "element_extreme_tet4": lambda: element_extreme_fixture(4),
+                "element_extreme_tet10": lambda: element_extreme_fixture(10, n=20)}
         for name in only:
             out[name] = gens[name]()
         for name, d in out.items():
@@ -352,6 +397,8 @@ def main(only=None):
     out["tet10_newton"] = tet10_newton_fixture()
     out["tet10_compress6"] = tet10_compress6_fixture()
     out["dynamic_tet10"] = dynamic_tet10_fixture()
+    out["element_extreme_tet4"] = element_extreme_fixture(4)
+    out["element_extreme_tet10"] = element_extreme_fixture(10, n=20)
 
     for name, d in out.items():
         path = os.path.join(HERE, f"{name}.npz")

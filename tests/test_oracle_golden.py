@@ -54,6 +54,29 @@ def test_vectorized_matches_reference_elements():
             assert rel_max(f[i], g["f"][i]) < 5e-12
 
 
+def test_oracle_matches_reference_at_extreme_states():
+    """Large stretch and compression with rotation (det F 0.35 to 2.5), Poisson ratios up
+    to 0.4999, and strains of 1e-7 (every fourth element), from the reference's element."""
+    for name, npe, mod in (("element_extreme_tet4", 4, tet4), ("element_extreme_tet10", 10, tet10)):
+        g = golden(name)
+        n = len(g["X"])
+        assert {0.35, 0.6, 1.8, 2.5} <= set(np.round(g["det_F"], 6)) and max(g["nu"]) == 0.4999
+        for i in range(n):
+            k, f = mod.force_and_tangent(g["X"][i], g["u"][i], g["mu"][i], g["kappa"][i])
+            assert rel_max(k, g["k"][i]) < 1e-15 and rel_max(f, g["f"][i]) < 1e-15  # step for step
+        nodes = g["X"].reshape(-1, 3)
+        els = np.arange(n * npe).reshape(n, npe)
+        k, f = vectorized.element_force_and_tangent(nodes, els, g["u"].reshape(-1, 3), g["mu"], g["kappa"])
+        for i in range(n):
+            assert rel_max(k[i], g["k"][i]) < 5e-13
+            if i % 4 == 3:
+                # strain 1e-7: the reference's S = phi (I - I1/3 C^-1) + beta C^-1 keeps
+                # about 1e-16 / 1e-7 of f, so another association agrees to ~1e-8 only
+                assert rel_max(f[i], g["f"][i]) < 2e-7
+            else:
+                assert rel_max(f[i], g["f"][i]) < 1e-12
+
+
 def test_cfg1_assembly_matches_reference():
     g = golden("cfg1_seeded")
     m = meshgen.box_tet4(1.0, 0.1, 0.1, 40, 4, 4)
