@@ -70,8 +70,9 @@ def test_oracle_matches_reference_at_extreme_states():
         for i in range(n):
             assert rel_max(k[i], g["k"][i]) < 5e-13
             if i % 4 == 3:
-                # strain 1e-7: the reference's S = phi (I - I1/3 C^-1) + beta C^-1 keeps
-                # about 1e-16 / 1e-7 of f, so another association agrees to ~1e-8 only
+                # strain 1e-7: the reference's S = phi (I - I1/3 C^-1) + beta C^-1 makes f
+                # accurate to about 1e-16 / 1e-7 = 1e-9 relative, so another association
+                # agrees to ~1e-8 only
                 assert rel_max(f[i], g["f"][i]) < 2e-7
             else:
                 assert rel_max(f[i], g["f"][i]) < 1e-12
