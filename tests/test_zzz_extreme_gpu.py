@@ -4,12 +4,11 @@ non-homogeneous part, Poisson ratios up to 0.4999, and strains of 1e-7 on every 
 element.
 
 Tolerances: K_T max-norm relative 1e-12 (FP64) and 2e-6 (FP32-mixed tangent); f_int
-1e-11, except at 1e-7 strain, where the reference's stress formula makes its f accurate
-to only about 1e-16 / 1e-7 = 1e-9 relative (the oracle's batched form, another association of the same formula,
-agrees with it to 3e-8 there), so the bar is 2e-7."""
+1e-11, except at 1e-7 strain, where the reference's stress formula makes its f
+accurate to only about 1e-16 / 1e-7 = 1e-9 relative (the oracle's batched form, another
+association of the same formula, agrees with it to 3e-8 there), so the bar is 2e-7."""
 from __future__ import annotations
 
-import numpy as np
 import pytest
 
 from conftest import block_diagonal_blocks, disjoint_mesh, golden, rel_max
