@@ -215,26 +215,44 @@ class DynamicRelaxationResult:
 
 class DynamicRelaxationAnalysis:
     def __init__(self, domain, damping_type: str = "kinetic", safety_factor: float = 1.1,
-                 viscous_damping: float | None = None, dt: float = 1.0) -> None:
+                 viscous_damping: float | None = None, dt: float = 1.0, mass: str = "gerschgorin") -> None:
+        """``mass``: "gerschgorin" (the reference's fictitious mass) or "lumped" (the row
+        sums of the domain's consistent mass matrix; see ``fictitious_mass``)."""
         self.domain = domain
         self.damping_type = damping_type.lower()
         if self.damping_type not in ("kinetic", "viscous"):
             raise ValueError(f"damping_type must be 'kinetic' or 'viscous', got '{damping_type}'")
+        self.mass = mass.lower()
+        if self.mass not in ("gerschgorin", "lumped"):
+            raise ValueError(f"mass must be 'gerschgorin' or 'lumped', got '{mass}'")
         self.safety_factor = float(safety_factor)
         self.viscous_damping = viscous_damping
         self.dt = float(dt)
 
     def fictitious_mass(self, dt: float, free, p_dofs):
-        """Gerschgorin diagonal mass of ``dynamic_relaxation.py:87-128`` (no contact)."""
+        """(diagonal mass, its inverse on the free DOFs, pseudo-time step).
+
+        "gerschgorin", the reference's (``dynamic_relaxation.py:87-128``, no contact):
+        m_i = sf dt^2 G_i / 4, with G_i the absolute row sum of the small-strain
+        stiffness, so that every mode is stable at the given dt.  "lumped" (a build
+        option; the reference has none): m_i = the row sum of the consistent mass matrix
+        (rho times volume per node), and the step becomes 2 / sqrt(sf max_i G_i / m_i)
+        over the free DOFs when dt is larger, the same stability margin."""
         K0 = self.domain.assemble_stiffness_matrix()
         rows = np.asarray(np.abs(K0).sum(axis=1)).ravel()
         mx = float(rows.max()) if rows.size and rows.max() > 0 else 1.0
         rows = np.maximum(rows, 1e-6 * mx)
-        m = 0.25 * self.safety_factor * dt ** 2 * rows
+        if self.mass == "lumped":
+            m = np.asarray(self.domain.assemble_mass_matrix().sum(axis=1), dtype=np.float64).ravel()
+            if not np.all(m[free] > 0.0):
+                raise ValueError("the lumped mass has a non-positive entry on a free DOF")
+            dt = min(dt, 2.0 / np.sqrt(self.safety_factor * float(np.max(rows[free] / m[free]))))
+        else:
+            m = 0.25 * self.safety_factor * dt ** 2 * rows
         inv = np.zeros_like(m)
         inv[free] = 1.0 / m[free]
         inv[p_dofs] = 0.0
-        return m, inv
+        return m, inv, dt
 
     def solve(self, dirichlet, f_ext=None, tol: float = 1e-5, max_steps: int = 5000, min_steps: int = 10,
               verbose: bool = False) -> DynamicRelaxationResult:
@@ -247,8 +265,7 @@ class DynamicRelaxationAnalysis:
         f = np.zeros(n) if f_ext is None else np.asarray(f_ext, dtype=np.float64).ravel()
         ref = float(np.linalg.norm(f[free]))
         ref = 1.0 if ref < 1e-12 else ref
-        dt = self.dt
-        m_diag, inv_m = self.fictitious_mass(dt, free, p_dofs)
+        m_diag, inv_m, dt = self.fictitious_mass(self.dt, free, p_dofs)
         u = dom.u.copy()
         u[p_dofs] = u_p
         v = np.zeros(n)

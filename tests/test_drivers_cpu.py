@@ -101,3 +101,66 @@ def test_concat_meshes_offsets_and_beam_batch_ranges():
         assert 0.5 <= c.length <= 2.0 and 1e3 <= c.youngs <= 1e6 and 0.3 <= c.poisson <= 0.49
         assert 10.0 <= c.traction[0] <= 1000.0 and c.traction[2] <= 0.0
         assert 400.0 * -c.traction[2] * c.length ** 2 / c.youngs <= 0.25 + 1e-12
+
+
+class MassSpringDomain(SpringDomain):
+    """SpringDomain with the small-strain stiffness and a diagonal mass, as the dynamic
+    relaxation driver needs them."""
+
+    def __init__(self, k=10.0, masses=(2.0, 1.0, 0.5)):
+        super().__init__(k)
+        self.masses = np.asarray(masses, dtype=np.float64)
+
+    def assemble_stiffness_matrix(self):
+        K = np.zeros((3, 3))
+        for i in range(2):
+            K[i:i + 2, i:i + 2] += self.k * np.array([[1, -1], [-1, 1]])
+        return spsp.csr_matrix(K)
+
+    def assemble_mass_matrix(self):
+        return spsp.diags(self.masses).tocsr()
+
+
+def _spring_dirichlet():
+    from psierra_b200.domain import DirichletConstraint
+
+    dm = DirichletManager(3)
+    dm.add_constraint(DirichletConstraint([0], components=(0,), value=0.0, dofs_per_node=1))
+    return dm
+
+
+@pytest.mark.parametrize("mass", ["gerschgorin", "lumped"])
+def test_dynamic_relaxation_mass_options_reach_the_equilibrium(mass):
+    from psierra_b200.analysis import DynamicRelaxationAnalysis
+
+    # a load at which the springs stiffen by 17%: within the margin of safety factor 2
+    # (the masses come from the small-strain stiffness)
+    f = np.array([0.0, 0.0, 2.5])
+    dr = DynamicRelaxationAnalysis(MassSpringDomain(), damping_type="viscous", viscous_damping=0.3, dt=1.0,
+                                   safety_factor=2.0, mass=mass)
+    r = dr.solve(_spring_dirichlet(), f_ext=f, tol=1e-10, max_steps=20000)
+    assert r.converged
+    e = np.diff(r.displacement)
+    assert np.allclose(10.0 * (e + e ** 3), 2.5, rtol=1e-8)
+
+
+def test_lumped_mass_takes_the_rows_of_the_mass_matrix_and_a_stable_step():
+    from psierra_b200.analysis import DynamicRelaxationAnalysis
+
+    dom = MassSpringDomain()
+    free, fixed = np.array([1, 2]), np.array([0])
+    rows = np.array([20.0, 40.0, 20.0])  # absolute row sums of the small-strain stiffness
+    for sf in (1.1, 2.0):
+        m, inv, dt = DynamicRelaxationAnalysis(dom, safety_factor=sf, dt=10.0, mass="lumped").fictitious_mass(
+            10.0, free, fixed)
+        assert np.array_equal(m, dom.masses) and inv[0] == 0.0 and np.allclose(inv[1:], 1.0 / dom.masses[1:])
+        # 2 / sqrt(sf max_free G_i / m_i): omega_max^2 dt^2 <= 4 / sf, the reference's margin
+        assert dt == pytest.approx(2.0 / np.sqrt(sf * max(rows[1] / 1.0, rows[2] / 0.5)))
+    # a step already below the bound is kept
+    _, _, dt = DynamicRelaxationAnalysis(dom, dt=0.01, mass="lumped").fictitious_mass(0.01, free, fixed)
+    assert dt == 0.01
+    # the reference's mass keeps the given step: m = sf dt^2 G / 4
+    m, _, dt = DynamicRelaxationAnalysis(dom, safety_factor=1.1, dt=1.0).fictitious_mass(1.0, free, fixed)
+    assert dt == 1.0 and np.allclose(m, 0.25 * 1.1 * rows)
+    with pytest.raises(ValueError, match="mass must be"):
+        DynamicRelaxationAnalysis(dom, mass="consistent")
