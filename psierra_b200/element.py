@@ -26,6 +26,27 @@ import torch
 from psierra_b200.assembler import GPUAssembler
 
 
+class DeviceCSR:
+    """A square CSR matrix whose arrays stay on the GPU: ``indptr`` and ``indices`` (int32,
+    the canonical pattern of ``coo_matrix(...).tocsr()``, shared by every call on the same
+    mesh) and ``data`` (this call's values: float64, or float32 for the FP32-mixed
+    tangent).  ``to_scipy()`` gives the float64 host matrix the parity-mode hooks return."""
+
+    def __init__(self, indptr: torch.Tensor, indices: torch.Tensor, data: torch.Tensor, shape) -> None:
+        self.indptr, self.indices, self.data, self.shape = indptr, indices, data, tuple(shape)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.data.numel())
+
+    def to_scipy(self) -> spsp.csr_matrix:
+        A = spsp.csr_matrix((self.data.double().cpu().numpy(), self.indices.cpu().numpy(),
+                             self.indptr.cpu().numpy()), shape=self.shape, copy=False)
+        A.has_sorted_indices = True
+        A.has_canonical_format = True
+        return A
+
+
 class _HostStaging:
     """Pinned host buffers for the per-call copies of u (in) and f / K values (out)."""
 
@@ -229,6 +250,20 @@ class _GPUElementBase:
         f, k = asm.assemble(u, want_f=True, want_k=True)
         return self._results.take(f), self._csr(k)
 
+    def assemble_force_and_tangent_device(self, mesh, displacement) -> tuple[torch.Tensor, DeviceCSR]:
+        """Throughput form of ``assemble_force_and_tangent``: f_int as a fresh float64
+        device tensor and K_T as a ``DeviceCSR`` over fresh device values, with nothing
+        copied back to the host.  ``displacement`` is a host array (uploaded) or a
+        float64 tensor on the assembler's device (used as it is)."""
+        asm = self._setup(mesh)
+        if isinstance(displacement, torch.Tensor):
+            u = displacement.reshape(-1)
+        else:
+            u = self._upload_u(displacement)
+        f, k = asm.assemble(u, want_f=True, want_k=True)
+        n = 3 * asm.n_nodes
+        return f, DeviceCSR(asm.dev["indptr"], asm.dev["indices"], k, (n, n))
+
     # ---------------------------------------------------------------- per-element API
     def compute_nonlinear_force_and_tangent_stiffness(self, node_coords, u_nodes, elem_index=None, **kw):
         """(k_tan, f_int) of one element (psierra ``element/tet4_total_lagrangian.py:77-139``).
@@ -393,6 +428,12 @@ class Tet4Fbar(_GPUElementBase):
         f, k = asm.assemble(self._upload_u(displacement), want_f=True, want_k=True)
         self._record_jbar()
         return self._download(f, "f"), asm.csr(k)
+
+    def assemble_force_and_tangent_device(self, mesh, displacement):
+        """Not offered: the reference's Tet4Fbar tangent is scipy's ``K_dev + K_vol``,
+        whose pattern drops the entries that sum to exactly zero, so it depends on the
+        values; this element returns it on the host only (``assemble_force_and_tangent``)."""
+        raise NotImplementedError("Tet4Fbar returns its value-dependent CSR pattern on the host only")
 
     def assemble_stiffness_matrix(self, mesh) -> spsp.csr_matrix:
         """The tangent at zero displacement (psierra ``tet4_fbar.py:241-246``)."""
